@@ -1,0 +1,378 @@
+#!/usr/bin/env python3
+"""Benchmark: one CheFSI pass (the eigensolver part of an SCF iteration) on Si216.
+
+Workload (the configuration the headline metric is quoted on): Si216, 3x3x3 conventional
+diamond supercell (30.78 Bohr cube), 90^3 grid (729,000 points), 520 states, FD order 12,
+Chebyshev degree 20, Gamma point, atoms displaced by seeded N(0, 0.02 Bohr).  The
+pseudopotential is the Si-like synthetic psp8 of lynx_b200.pseudo and V_eff a seeded
+synthetic potential (no converged Si216 potential or Si psp8 is available), so `data` is
+"synthetic".
+
+A step = one CheFSI pass = Chebyshev filter (20 H-applies) + H*Y + Rayleigh-Ritz
+(overlap, projected H, Cholesky, subspace eigensolve, rotation) on device-resident
+orbitals; value = seconds per pass (lower is better).  With --gpus N each rank runs its
+own replica (the path has no exchange step: replicas only); the timing is the max over
+ranks.  `--impl reference` times the reference's own CPU code (oracle/_ref) on a bounded
+sample of the same workload on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s/SCF-iter Si216 CheFSI: mixed vs plain FP64 on B200 at ΔE≤1e-5 Ha/atom; HBM GB/s"
+
+CONFIGS = {
+    # name: (reps, grid, nstates, degree, displace)
+    "si216": (3, 90, 520, 20, 0.02),
+    "si64": (2, 60, 160, 20, 0.0),
+    "si8": (1, 30, 24, 20, 0.0),
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="lynx", choices=["lynx", "reference"])
+    p.add_argument("--config", default="si216", choices=sorted(CONFIGS))
+    p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def build_system(config, seed=2024):
+    from lynx_b200 import cell as C
+    from lynx_b200 import pseudo as P
+    reps, grid, nst, degree, disp = CONFIGS[config]
+    cl, pos = C.diamond_si(reps, grid, displace=disp, seed=seed)
+    psp_path = os.path.join("/tmp", f"lynx_b200_si_synthetic_{os.getpid()}.psp8")
+    P.synthetic_si_psp8(psp_path)
+    psp = P.read_psp8(psp_path)
+    tab = P.nonlocal_tables(cl, pos, psp)
+    V = veff_separable(cl, pos, noise=1e-3, seed=seed)
+    return cl, pos, psp_path, tab, V, nst, degree
+
+
+def veff_separable(cl, pos, depth=1.2, width=1.1, noise=0.0, seed=0):
+    """Same potential as lynx_b200.cell.synthetic_veff for orthogonal cells, evaluated
+    separably (sum over atoms of products of periodic 1-D Gaussians)."""
+    nx, ny, nz = cl.shape
+    h = cl.spacing
+    L = cl.lengths
+    axes = [np.arange(n) * h[d] for d, n in enumerate((nx, ny, nz))]
+    V = np.zeros((nz, ny, nx))
+    for p in pos:
+        g = []
+        for d in range(3):
+            x = axes[d][:, None] - p[d] - L[d] * np.arange(-2, 3)[None, :]
+            g.append(np.exp(-x * x / (2 * width * width)).sum(1))
+        V -= depth * np.einsum("k,j,i->kji", g[2], g[1], g[0])
+    V = V.ravel()
+    if noise > 0:
+        V += np.random.default_rng(seed).normal(0.0, noise, size=V.shape)
+    return V
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), float(d.get("bf16_tflops", 1590.0)), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+def cpu_baseline_sample(cl, pos, psp_path, V, nstates, degree, cols=8):
+    """Reference CPU CheFSI time per pass, estimated from a bounded sample.
+
+    filter: the reference chebyshev_filter on `cols` of the columns, scaled by nstates/cols
+    (the filter is column-independent);  Rayleigh-Ritz: the reference orthogonalize +
+    project + diag + rotate on all nstates columns of a 1/8-size grid (45^3 for Si216), the
+    grid-proportional part scaled by 8 and the N^3 eigensolve counted once."""
+    from lynx_b200 import cell as C
+    from oracle import ref
+    nthreads = os.cpu_count() or 1
+    ref.set_threads(nthreads)
+    R = ref.RefLynx(cl, pos, psp_path)
+    lo, hi = R.lanczos(V, maxit=60)
+    lc = 0.5 * (lo + hi)
+    X = C.random_orbitals(R.nd, cols, seed=7)
+    t0 = time.perf_counter()
+    R.chebyshev_filter(X, V, lc, lo, hi, degree)
+    t_filter = (time.perf_counter() - t0) * nstates / cols
+    # Rayleigh-Ritz on a coarser grid with all states
+    from lynx_b200.cell import Cell
+    g = tuple(max(13, n // 2) for n in cl.shape)
+    cs = Cell(cl.latvec, g, True, (0, 0, 0), cl.fd_order)
+    Rs = ref.RefLynx(cs, pos, psp_path)
+    scale = float(np.prod(cl.shape)) / float(np.prod(g))
+    Vs = veff_separable(cs, pos)
+    Y = C.random_orbitals(Rs.nd, nstates, seed=8)
+    t0 = time.perf_counter()
+    Yo = Rs.orthogonalize(Y)
+    Hs = Rs.project(Yo, Vs)
+    t1 = time.perf_counter()
+    eig, Q = Rs.diag(Hs)
+    t2 = time.perf_counter()
+    Rs.rotate(Yo, Q)
+    t3 = time.perf_counter()
+    t_rr = ((t1 - t0) + (t3 - t2)) * scale + (t2 - t1)
+    ref.lib().ref_free()
+    total = t_filter + t_rr
+    sample = (f"reference CPU CheFSI (oracle/_ref, OpenMP {nthreads} threads): filter degree {degree} on "
+              f"{cols}/{nstates} columns of the {cl.shape[0]}^3 grid scaled x{nstates / cols:.1f}; "
+              f"Rayleigh-Ritz on all {nstates} states of a {g[0]}^3 grid, grid-proportional part scaled "
+              f"x{scale:.2f}, eigensolve once")
+    return total, nthreads, sample, {"filter_s": t_filter, "rr_s": t_rr}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_lynx.so not built"}))
+        return
+    cl, pos, psp_path, tab, V, nst, degree = build_system(args.config)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t, cores, sample, parts = cpu_baseline_sample(cl, pos, psp_path, V, nst, degree)
+        if i >= args.warmup:
+            times.append(t)
+    v = float(np.mean(times))
+    line = {
+        "metric": METRIC, "value": v, "unit": "s/iter", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{args.config} CheFSI pass", "grid": cl.shape[0], "nstates": nst,
+                   "degree": degree, "fd_order": 12, "parallelism": "replicas"},
+        "cpu_baseline": {"value": v, "unit": "s/iter", "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": v, "unit": "s/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from lynx_b200 import _lib
+    from lynx_b200 import solver
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    cl, pos, psp_path, tab, V, nst, degree = build_system(args.config)
+    ctx = solver.Context(cl, device=local)
+    ctx.set_nonlocal(tab)
+    lib = ctx.lib
+    Vd = torch.from_numpy(V).cuda()
+    es = solver.EigenSolver(ctx, args.precision)
+    lo, hi = es.lanczos_bounds(Vd)
+    lc, emin = 0.5 * (lo + hi), lo
+    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    psi = (torch.rand((nst, ctx.nd), generator=gen, device="cuda", dtype=torch.float64) - 0.5).contiguous()
+
+    def one_pass(precision):
+        nonlocal lc, emin
+        _, eig = es.solve(psi, Vd, lc, emin, hi, degree, precision=precision)
+        lc = es.lambda_cutoff()
+        emin = float(eig[0])
+        return eig
+
+    for _ in range(args.warmup):
+        one_pass(args.precision)
+    # accuracy check on the warmed-up subspace: one pass in each precision from the same state
+    psi_save = psi.clone()
+    st = (lc, emin)
+    eig_fp64 = one_pass("fp64")
+    psi.copy_(psi_save)
+    lc, emin = st
+    eig_mixed = one_pass("mixed")
+    psi.copy_(psi_save)
+    lc, emin = st
+    del psi_save
+    natom = len(pos)
+    nocc = 2 * natom  # 4 valence electrons per Si, 2 per state
+    acc = {"max_abs_dE_occ_Ha": float(np.abs(eig_mixed[:nocc] - eig_fp64[:nocc]).max()),
+           "band_energy_dE_per_atom_Ha": float(abs(2.0 * (eig_mixed[:nocc] - eig_fp64[:nocc]).sum()) / natom)}
+
+    # FP64 timing (the plain-FP64 GPU CheFSI the mixed path is compared against)
+    def timed(precision, k):
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(k):
+            one_pass(precision)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / k
+
+    other = "fp64" if args.precision == "mixed" else "mixed"
+    t_other = timed(other, max(1, min(2, args.steps)))
+
+    lib.lynx_launch_count(1)
+    with ClockSampler(local) as clk:
+        t_main = timed(args.precision, args.steps)
+    launches = int(lib.lynx_launch_count(1))
+    t = torch.tensor([t_main], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_main = float(t.item())
+
+    # Roofline of the dominant kernel: the fused Chebyshev step, timed alone with CUDA events.
+    import ctypes
+    ms = ctypes.c_double()
+    prec_id = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
+    ctx.sync_stream()
+    _lib.check(lib.lynx_time_filter_step(ctx.handle, ctypes.c_void_p(Vd.data_ptr()), nst, prec_id, 0, 10,
+                                         ctypes.byref(ms)))
+    ms_nl = ctypes.c_double()
+    _lib.check(lib.lynx_time_filter_step(ctx.handle, ctypes.c_void_p(Vd.data_ptr()), nst, prec_id, 1, 5,
+                                         ctypes.byref(ms_nl)))
+    wsize = 4 if args.precision == "mixed" else 8
+    step_bytes = wsize * ctx.nd * (3 * nst + 1)  # x, xold, out per update + V per point
+    hbm, bf16, peak_kind = measured_peaks()
+    achieved = step_bytes / (ms.value * 1e-3) / 1e9
+    updates = ctx.nd * nst * degree
+
+    e2e = None
+    if not args.no_e2e:
+        host_psi = torch.empty((nst, ctx.nd), dtype=torch.float64, pin_memory=True)
+        host_psi.copy_(psi)
+        hv = torch.from_numpy(V).pin_memory()
+        eig = np.zeros(nst)
+        lc_out = ctypes.c_double()
+        hp = host_psi.numpy()
+        hvn = hv.numpy()
+        _lib.check(lib.lynx_eigensolver_solve_host(ctx.handle, _lib.dptr(hp), _lib.dptr(eig), _lib.dptr(hvn), nst,
+                                                   ctx.nd, lc, emin, hi, degree, prec_id, ctypes.byref(lc_out)))
+        torch.cuda.synchronize()
+        k = max(1, min(3, args.steps))
+        t0 = time.perf_counter()
+        for _ in range(k):
+            _lib.check(lib.lynx_eigensolver_solve_host(ctx.handle, _lib.dptr(hp), _lib.dptr(eig), _lib.dptr(hvn),
+                                                       nst, ctx.nd, lc_out.value, float(eig[0]), hi, degree,
+                                                       prec_id, ctypes.byref(lc_out)))
+        torch.cuda.synchronize()
+        te = (time.perf_counter() - t0) / k
+        e2e = {"value": te, "unit": "s/iter", "h2d_bytes_per_step": int(8 * ctx.nd * (nst + 1)),
+               "d2h_bytes_per_step": int(8 * (ctx.nd * nst + nst)), "api": "lynx_eigensolver_solve_host"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import ref
+        if ref.available():
+            v, cores, sample, parts = cpu_baseline_sample(cl, pos, psp_path, V, nst, degree)
+            cpu = {"value": v, "unit": "s/iter", "cores": cores, "kind": "reference", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": t_main, "unit": "s/iter", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_main * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": f"{args.config} CheFSI pass ({args.precision})", "grid": cl.shape[0],
+                       "nstates": nst, "degree": degree, "fd_order": 12, "natom": natom,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (orbital blocks of %.2f GB)" % (wsize * ctx.nd * nst / 1e9)},
+            "updates_per_s": world * updates / t_main,
+            "fp64_s_per_iter" if args.precision == "mixed" else "mixed_s_per_iter": t_other,
+            "speedup_vs_fp64" if args.precision == "mixed" else "speedup_vs_mixed": t_other / t_main,
+            "accuracy": acc,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "traffic": None, "kernel": "cheb_step_kernel (fused stencil+Veff+recurrence)",
+                         "ms_per_launch": ms.value, "ms_per_step_with_nonlocal": ms_nl.value,
+                         "peak_kind": peak_kind},
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    try:
+        os.remove(psp_path)
+    except OSError:
+        pass
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,191 @@
+/*
+ * lynx_b200 — C ABI of the B200-native CheFSI eigensolver hot path.
+ *
+ * Every entry point replaces one reference LYNX interface (cited per function,
+ * paths relative to the LYNX source tree).  The ABI uses plain pointers, sizes
+ * and status codes only: no C++ or torch types cross it.
+ *
+ * Conventions (same as the reference):
+ *   - Orbitals are column-major Nd x ncol blocks, column stride `ld` >= Nd
+ *     (ld = 0 means ld = Nd), grid index i + j*nx + k*nx*ny (x fastest).
+ *   - Complex (k-point) arrays are interleaved (re, im) doubles, like
+ *     std::complex<double>.
+ *   - Operator entry points take DEVICE pointers and run on the context's
+ *     stream (lynx_set_stream).  The *_host entry points take host pointers.
+ *   - Every call returns LYNX_OK or an error status; lynx_last_error() gives
+ *     the message of the last failing call on the calling thread.  Nothing
+ *     calls exit(): a CUDA or solver failure is reported, not fatal.
+ *   - A context is not re-entrant: calls on one context must not overlap.
+ *     Different contexts are independent (no process-wide coefficient caches).
+ */
+#ifndef LYNX_B200_H
+#define LYNX_B200_H
+
+#if defined(__GNUC__)
+#define LYNX_API __attribute__((visibility("default")))
+#else
+#define LYNX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes (the reference throws std::runtime_error or exit()s instead,
+ * src/solvers/EigenSolver.cpp:633-635,667-670; src/core/gpu_common.cuh:8-15). */
+enum {
+    LYNX_OK = 0,
+    LYNX_ERR_BAD_ARG = 1,
+    LYNX_ERR_CUDA = 2,
+    LYNX_ERR_OOM = 3,
+    LYNX_ERR_CHOL_FAIL = 4,  /* overlap matrix not positive definite (potrf info > 0) */
+    LYNX_ERR_EIG_FAIL = 5,   /* subspace eigensolver did not converge (syev info > 0) */
+    LYNX_ERR_NONFINITE = 6,  /* NaN/Inf in the eigenvalues or the subspace matrices */
+    LYNX_ERR_TIMEOUT = 7,    /* a bounded device-side wait gave up */
+    LYNX_ERR_NOT_SETUP = 8,
+    LYNX_ERR_UNSUPPORTED = 9,
+    LYNX_ERR_BRACKET = 10    /* Fermi level cannot be bracketed */
+};
+
+/* Arithmetic of the CheFSI pass. */
+enum {
+    LYNX_PREC_FP64 = 0,  /* plain FP64 everywhere */
+    LYNX_PREC_MIXED = 1  /* FP32 filter + BF16x3 tensor-core Rayleigh-Ritz products, FP64 subspace algebra */
+};
+
+enum { LYNX_BC_PERIODIC = 0, LYNX_BC_DIRICHLET = 1 };
+enum { LYNX_SMEAR_GAUSSIAN = 0, LYNX_SMEAR_FERMI_DIRAC = 1 };
+
+typedef struct lynx_ctx lynx_ctx;
+
+LYNX_API const char* lynx_status_string(int status);
+LYNX_API const char* lynx_last_error(void);
+LYNX_API int lynx_version(void);
+
+/* Grid, lattice and FD stencil of one cell on one device.
+ * Replaces FDGrid(Nx,Ny,Nz,lattice,bc...) (src/core/FDGrid.hpp:11-12),
+ * Lattice(latvec, cell_type) (src/core/Lattice.hpp:10),
+ * FDStencil(order, grid, lattice) (src/operators/FDStencil.hpp:12),
+ * HaloExchange(domain, FDn) (src/parallel/HaloExchange.hpp:21) and
+ * Hamiltonian::setup / setup_gpu (src/operators/Hamiltonian.hpp:50-54,119-123).
+ *   latvec: 3x3 row-major, rows are the lattice vectors (Bohr).
+ *   orthogonal: 1 for CellType::Orthogonal, 0 for NonOrthogonal.
+ *   bc: 3 ints, LYNX_BC_PERIODIC or LYNX_BC_DIRICHLET per direction (NULL = periodic). */
+LYNX_API int lynx_create(lynx_ctx** out, int device, int nx, int ny, int nz, int fd_order, const double* latvec,
+                int orthogonal, const int* bc);
+LYNX_API int lynx_destroy(lynx_ctx* ctx);
+
+/* CUDA stream (cudaStream_t) for all later work on this context; NULL = the legacy default stream. */
+LYNX_API int lynx_set_stream(lynx_ctx* ctx, void* stream);
+
+/* Nd, dV (FDGrid::dV, src/core/FDGrid.cpp:33) and the largest eigenvalue of -0.5*Lap
+ * (FDStencil::max_eigval_half_lap, src/operators/FDStencil.cpp:154-180). */
+LYNX_API int lynx_grid_info(const lynx_ctx* ctx, int* nd, double* dV, double* max_eigval_half_lap);
+
+/* Scaled stencil coefficients, FDn+1 doubles each (any pointer may be NULL):
+ * FDStencil::D2_coeff_{x,y,z}, D2_coeff_{xy,xz,yz}, D1_coeff_{x,y,z} (src/operators/FDStencil.hpp:19-31). */
+LYNX_API int lynx_stencil_coeffs(const lynx_ctx* ctx, double* d2x, double* d2y, double* d2z, double* d2xy,
+                        double* d2xz, double* d2yz, double* d1x, double* d1y, double* d1z);
+
+/* Nonlocal projector tables, in the flattened form the reference uploads in
+ * Hamiltonian::setup_gpu (src/operators/Hamiltonian.cu:342-495) from
+ * NonlocalProjector::setup (src/operators/NonlocalProjector.cpp:13-119) and
+ * Crystal::compute_nloc_influence (src/atoms/Crystal.cpp:136-255):
+ *   n_img images of atoms whose rc-sphere meets the cell; image i belongs to
+ *   physical atom img_atom[i], covers img_ndc[i] grid points listed in gpos
+ *   (concatenated over images), has lattice shift img_shift[3i..3i+2] (Bohr,
+ *   AtomNlocInfluence::image_shift) and projector values chi (concatenated over
+ *   images, each block img_ndc[i] x atom_nproj[img_atom[i]] column-major).
+ *   gamma: KB energies per (atom, projector) in atom order.
+ * Host pointers; the tables are copied to the device. n_img = 0 clears them. */
+LYNX_API int lynx_set_nonlocal(lynx_ctx* ctx, int n_img, const int* img_atom, const int* img_ndc,
+                      const double* img_shift, const int* gpos, const double* chi, int n_atom,
+                      const int* atom_nproj, const double* gamma);
+
+/* Bloch vector for the *_kpt entry points, in the reference's k-point units
+ * (KPoints::kpts_cart, src/core/KPoints.cpp:49-52; ghost phase e^{+-i k_d L_d},
+ * src/parallel/HaloExchange.cpp:121-133; projector phase e^{-i k.R_image},
+ * src/operators/NonlocalProjector.cpp:253-257).
+ * Replaces Hamiltonian::set_kpoint_gpu (src/operators/Hamiltonian.hpp:129) and
+ * NonlocalProjector::set_kpoint (src/operators/NonlocalProjector.hpp:57). */
+LYNX_API int lynx_set_kpoint(lynx_ctx* ctx, const double* kpt_cart);
+
+/* y = H psi + c psi, H = -0.5 Lap + Veff + Vnl.  Device pointers; veff is Nd doubles.
+ * Replaces Hamiltonian::apply (src/operators/Hamiltonian.hpp:64-65) / apply_gpu (:137). */
+LYNX_API int lynx_hamiltonian_apply(lynx_ctx* ctx, const double* psi, const double* veff, double* y, int ncol, int ld,
+                           double c);
+
+/* Complex k-point version. Replaces Hamiltonian::apply_kpt (src/operators/Hamiltonian.hpp:78-80). */
+LYNX_API int lynx_hamiltonian_apply_kpt(lynx_ctx* ctx, const double* psi_z, const double* veff, double* y_z, int ncol,
+                               int ld, double c);
+
+/* hpsi += Vnl psi.  Replaces NonlocalProjector::apply / apply_kpt
+ * (src/operators/NonlocalProjector.hpp:47,51). */
+LYNX_API int lynx_nonlocal_apply(lynx_ctx* ctx, const double* psi, double* hpsi, int ncol, int ld);
+LYNX_API int lynx_nonlocal_apply_kpt(lynx_ctx* ctx, const double* psi_z, double* hpsi_z, int ncol, int ld);
+
+/* Chebyshev filter of degree `degree`: Y = p_m(H) X with the reference's scaled three-term
+ * recurrence.  Replaces EigenSolver::chebyshev_filter_impl (src/solvers/EigenSolver.cpp:559-619)
+ * and chebyshev_filter_gpu (src/solvers/EigenSolver.cu:755-783).  `precision` selects FP64 or
+ * the FP32 filter; input and output stay FP64. */
+LYNX_API int lynx_chebyshev_filter(lynx_ctx* ctx, const double* X, double* Y, const double* veff, int ncol, int ld,
+                          double lambda_cutoff, double eigmin, double eigmax, int degree, int precision);
+LYNX_API int lynx_chebyshev_filter_kpt(lynx_ctx* ctx, const double* X_z, double* Y_z, const double* veff, int ncol,
+                              int ld, double lambda_cutoff, double eigmin, double eigmax, int degree,
+                              int precision);
+
+/* One CheFSI pass on device-resident orbitals: filter -> Cholesky-QR -> project -> subspace
+ * eigensolve -> rotate.  psi (device, in/out) is overwritten by the Ritz vectors; eig (HOST,
+ * nband doubles) receives the Ritz values in ascending order; *lambda_cutoff_out (may be NULL)
+ * receives eig[nband-1] + 0.1 (the reference's next cutoff, src/solvers/EigenSolver.cpp:817).
+ * Replaces EigenSolver::solve_resident (src/solvers/EigenSolver.hpp:101-104) and, with host
+ * data, EigenSolver::solve (:38-41). */
+LYNX_API int lynx_eigensolver_solve(lynx_ctx* ctx, double* psi, double* eig, const double* veff, int nband, int ld,
+                           double lambda_cutoff, double eigmin, double eigmax, int degree, int precision,
+                           double* lambda_cutoff_out);
+
+/* Complex k-point CheFSI pass at the context's k-point (lynx_set_kpoint).
+ * Replaces EigenSolver::solve_kpt / solve_kpt_resident (src/solvers/EigenSolver.hpp:49-53,107-110). */
+LYNX_API int lynx_eigensolver_solve_kpt(lynx_ctx* ctx, double* psi_z, double* eig, const double* veff, int nband,
+                               int ld, double lambda_cutoff, double eigmin, double eigmax, int degree,
+                               int precision, double* lambda_cutoff_out);
+
+/* Host-pointer CheFSI pass: EigenSolver::solve (src/solvers/EigenSolver.hpp:38-41) exactly as the
+ * CPU caller uses it (psi, eig, Veff in host memory).  Copies in, solves on the device, copies out. */
+LYNX_API int lynx_eigensolver_solve_host(lynx_ctx* ctx, double* psi, double* eig, const double* veff, int nband,
+                                int ld, double lambda_cutoff, double eigmin, double eigmax, int degree,
+                                int precision, double* lambda_cutoff_out);
+
+/* Extreme eigenvalue estimates of H by Lanczos (tolerance on both ends, at most max_iter steps,
+ * fixed seed), returned with the reference's safety margins (max*1.01, min-0.1).  Device veff.
+ * Replaces EigenSolver::lanczos_bounds / lanczos_bounds_kpt (src/solvers/EigenSolver.hpp:43-45,55-58;
+ * src/solvers/Lanczos.hpp:92-200). */
+LYNX_API int lynx_lanczos_bounds(lynx_ctx* ctx, const double* veff, double tol, int max_iter, double* eigmin,
+                        double* eigmax);
+LYNX_API int lynx_lanczos_bounds_kpt(lynx_ctx* ctx, const double* veff, double tol, int max_iter, double* eigmin,
+                            double* eigmax);
+
+/* Fermi level by Brent's method on sum_i w_i f(eps_i - Ef) = nelectron (tolerance 1e-14, <= 200
+ * iterations), f Fermi-Dirac or Gaussian smearing.  Host arrays, FP64.
+ * Replaces Occupation::find_fermi_level (src/electronic/Occupation.cpp:48-84). */
+LYNX_API int lynx_fermi_level(const double* eigs, const double* weights, int n, double nelectron, double beta,
+                     int smearing, double* ef);
+
+/* occ[i] = f(eigs[i] - ef).  Replaces the occupation loop of Occupation::compute
+ * (src/electronic/Occupation.cpp:208-218) and Occupation::smearing_function (:26-35). */
+LYNX_API int lynx_occupations(const double* eigs, int n, double ef, double beta, int smearing, double* occ);
+
+/* Diagnostic, no counterpart in the reference: device time of one Chebyshev degree step
+ * (out = a*H*x + b*x + d*xold over ncol columns of this context's grid, with or without the
+ * nonlocal gather/scatter), averaged over `reps` back-to-back steps on the context's work
+ * buffers and timed with CUDA events on the context's stream. */
+LYNX_API int lynx_time_filter_step(lynx_ctx* ctx, const double* veff, int ncol, int precision, int with_nonlocal,
+                                   int reps, double* ms_per_step);
+
+/* Number of kernel launches this library issued since the last reset (diagnostic counter). */
+LYNX_API long long lynx_launch_count(int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LYNX_B200_H */

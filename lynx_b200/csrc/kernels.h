@@ -1,0 +1,63 @@
+// Host-side launch interfaces of the lynx_b200 kernels (implemented in the .cu files).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace lynxb {
+
+// Geometry + FD coefficients of one cell for the fused stencil kernel.
+struct StencilGeom {
+    int nx, ny, nz;
+    int R;               // FD half-width
+    const double* D2x;   // FDn+1 scaled second-derivative coefficients (host)
+    const double* D2y;
+    const double* D2z;
+};
+
+// out = a*(-0.5*Lap x + V.*x) + b*x + d*xold over ncol columns (xold may be null when d == 0).
+// phl/phr: per-direction ghost multipliers (3 values of T each).
+template <typename T, typename S>
+int launch_cheb_step(const StencilGeom& g, const T* x, long long ldx, const T* xold, long long ldo, T* out,
+                     long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl,
+                     const T* phr, cudaStream_t st);
+
+// Launches issued by the library (diagnostic counter, incremented by every launcher).
+void count_launch(int n = 1);
+
+}  // namespace lynxb
+
+namespace lynxb {
+
+// Device copy of the nonlocal projector tables (see nonlocal.cuh for the layout).
+struct NLDev {
+    int n_atom = 0, n_img = 0, n_pts = 0, max_np = 0, total_proj = 0;
+    int* atom_img_ptr = nullptr;
+    int* atom_img_list = nullptr;
+    int* atom_nproj = nullptr;
+    int* atom_poff = nullptr;
+    double* gamma = nullptr;
+    int* img_atom = nullptr;
+    int* img_ndc = nullptr;
+    long long* img_goff = nullptr;
+    long long* img_chi_off = nullptr;
+    double* img_phase = nullptr;
+    int* gpos = nullptr;
+    double* chi64 = nullptr;
+    float* chi32 = nullptr;
+    int* pt_grid = nullptr;
+    int* pt_ptr = nullptr;
+    int* ent_img = nullptr;
+    int* ent_loc = nullptr;
+};
+
+// Column block widths of the nonlocal kernels; alpha rows are padded to a multiple of kNLColBlock.
+constexpr int kNLColBlock = 16;
+
+template <typename T>
+int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alpha, int ncolp, double dV,
+                     cudaStream_t st);
+template <typename T, typename S>
+int launch_nl_scatter(const NLDev& nl, T* out, long long ld, int ncol, const T* alpha, int ncolp, S scale,
+                      cudaStream_t st);
+
+}  // namespace lynxb

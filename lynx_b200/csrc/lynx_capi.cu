@@ -1,0 +1,1277 @@
+// C ABI of lynx_b200: context set-up, operator entry points and the CheFSI driver.
+//
+// The driver mirrors EigenSolver::solve_impl (src/solvers/EigenSolver.cpp:739-818):
+//   filter (degree m)  ->  Cholesky-QR  ->  project  ->  subspace eigensolve  ->  rotate,
+// with two B200-specific changes that keep the arithmetic identical:
+//   * the three filter buffers rotate by pointer (the reference GPU path copies
+//     two full blocks per degree step, src/solvers/EigenSolver.cu:190-191);
+//   * the Cholesky factor R of the overlap is folded into the subspace matrix and
+//     the rotation, Hs' = R^-T Hs R^-1 and psi = Y (R^-1 Q), which equals the
+//     reference's Y <- Y R^-1; Hs = dV Y^T H Y; psi = Y Q, but needs no pass of
+//     trsm over the Nd x N block and lets H*Y run on the unorthogonalised Y.
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "lynx_common.cuh"
+#include "stencil.cuh"
+
+namespace lynxb {
+
+static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Growable device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t b) {
+        if (b <= bytes) return LYNX_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc(%zu) failed: %s", b, cudaGetErrorString(e));
+            return LYNX_ERR_OOM;
+        }
+        bytes = b;
+        return LYNX_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------------------
+// Elementwise helper kernels
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cvt_val(double& d, float s) { d = (double)s; }
+__device__ __forceinline__ void cvt_val(float& d, double s) { d = (float)s; }
+__device__ __forceinline__ void cvt_val(double& d, double s) { d = s; }
+__device__ __forceinline__ void cvt_val(float& d, float s) { d = s; }
+__device__ __forceinline__ void cvt_val(double2& d, float2 s) { d = make_double2(s.x, s.y); }
+__device__ __forceinline__ void cvt_val(float2& d, double2 s) { d = make_float2((float)s.x, (float)s.y); }
+__device__ __forceinline__ void cvt_val(double2& d, double2 s) { d = s; }
+
+template <typename Dst, typename Src>
+__global__ void convert_cols_kernel(Dst* __restrict__ dst, long long ldd, const Src* __restrict__ src,
+                                    long long lds, long long nrow, int ncol) {
+    const long long total = nrow * ncol;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long c = i / nrow, r = i - c * nrow;
+        cvt_val(dst[c * ldd + r], src[c * lds + r]);
+    }
+}
+
+template <typename Dst, typename Src>
+int convert_cols(Dst* dst, long long ldd, const Src* src, long long lds, long long nrow, int ncol,
+                 cudaStream_t st) {
+    const long long total = nrow * ncol;
+    if (total == 0) return LYNX_OK;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+    convert_cols_kernel<Dst, Src><<<blocks, 256, 0, st>>>(dst, ldd, src, lds, nrow, ncol);
+    count_launch();
+    LYNX_CUDA_TRY(cudaGetLastError());
+    return LYNX_OK;
+}
+
+// Symmetrise (real) / Hermitise (complex) an N x N column-major matrix in place.
+__global__ void symmetrize_kernel(double* A, int N) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i < j && j < N) {
+        const double v = 0.5 * (A[i + (long long)j * N] + A[j + (long long)i * N]);
+        A[i + (long long)j * N] = v;
+        A[j + (long long)i * N] = v;
+    }
+}
+__global__ void hermitize_kernel(double2* A, int N) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i < N && j < N) {
+        if (i < j) {
+            const double2 a = A[i + (long long)j * N], b = A[j + (long long)i * N];
+            const double2 v = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+            A[i + (long long)j * N] = v;
+            A[j + (long long)i * N] = make_double2(v.x, -v.y);
+        } else if (i == j) {
+            A[i + (long long)i * N].y = 0.0;
+        }
+    }
+}
+
+}  // namespace lynxb
+
+using namespace lynxb;
+
+// ---------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------
+struct lynx_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int nx = 0, ny = 0, nz = 0, Nd = 0, fd_order = 0, R = 0;
+    bool orth = true;
+    int bc[3] = {0, 0, 0};
+    double latvec[9] = {0}, uvec[9] = {0}, lapcT[9] = {0}, L[3] = {0, 0, 0};
+    double jac = 0, dx = 0, dy = 0, dz = 0, dV = 0, maxeig = 0;
+    std::vector<double> w1, w2, D2x, D2y, D2z, D1x, D1y, D1z, D2xy, D2xz, D2yz;
+    double kpt[3] = {0, 0, 0};
+    // nonlocal
+    bool has_nl = false;
+    NLDev nl;
+    std::vector<DevBuf> nl_bufs;
+    std::vector<double> img_shift;  // host copy for phase updates
+    // handles
+    cublasHandle_t cublas = nullptr;
+    cusolverDnHandle_t cusolver = nullptr;
+    // work buffers
+    DevBuf wbuf[4];       // filter / RR blocks (any precision)
+    DevBuf cvt[2];        // FP64 copies of FP32 blocks for the Rayleigh-Ritz products
+    DevBuf alpha;         // nonlocal projections
+    DevBuf v32;           // FP32 copy of Veff
+    DevBuf Ms, Hs, eigd, solver_work, info;
+    DevBuf lz[4];         // Lanczos vectors
+    DevBuf io_psi, io_v;  // staging for the host-pointer solve
+};
+
+namespace {
+
+int activate(lynx_ctx* c) {
+    LYNX_CUDA_TRY(cudaSetDevice(c->device));
+    return LYNX_OK;
+}
+
+double fract(int n, int k) {
+    // n! / ((n-k)! (n+k)!)
+    double num = 1.0, den = 1.0;
+    for (int i = n - k + 1; i <= n; ++i) num *= i;
+    for (int i = n + 1; i <= n + k; ++i) den *= i;
+    return num / den;
+}
+
+void mat3_inverse(const double* a, double* inv) {
+    const double det = a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]);
+    inv[0] = (a[4] * a[8] - a[5] * a[7]) / det;
+    inv[1] = (a[2] * a[7] - a[1] * a[8]) / det;
+    inv[2] = (a[1] * a[5] - a[2] * a[4]) / det;
+    inv[3] = (a[5] * a[6] - a[3] * a[8]) / det;
+    inv[4] = (a[0] * a[8] - a[2] * a[6]) / det;
+    inv[5] = (a[2] * a[3] - a[0] * a[5]) / det;
+    inv[6] = (a[3] * a[7] - a[4] * a[6]) / det;
+    inv[7] = (a[1] * a[6] - a[0] * a[7]) / det;
+    inv[8] = (a[0] * a[4] - a[1] * a[3]) / det;
+}
+
+// Central-difference weights of order 2*FDn (Fornberg), scaled to the grid and,
+// for non-orthogonal cells, to the Laplacian metric lapc_T = (U^-1)^T U^-1 of the
+// unit lattice vectors U (the conventions of src/operators/FDStencil.cpp:73-152
+// and src/core/Lattice.cpp:13-51).
+void build_stencil(lynx_ctx* c) {
+    const int n = c->R + 1;
+    c->w1.assign(n, 0.0);
+    c->w2.assign(n, 0.0);
+    for (int p = 1; p < n; ++p) {
+        const double sgn = (p % 2 == 1) ? 1.0 : -1.0;
+        c->w1[p] = sgn * fract(c->R, p) / p;
+        c->w2[0] -= 2.0 / ((double)p * p);
+        c->w2[p] = sgn * 2.0 * fract(c->R, p) / ((double)p * p);
+    }
+    // lattice
+    for (int i = 0; i < 3; ++i) {
+        double len = 0;
+        for (int j = 0; j < 3; ++j) len += c->latvec[3 * i + j] * c->latvec[3 * i + j];
+        len = std::sqrt(len);
+        c->L[i] = len;
+        for (int j = 0; j < 3; ++j) c->uvec[3 * i + j] = c->latvec[3 * i + j] / len;
+    }
+    const double* a = c->latvec;
+    c->jac = std::fabs(a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+                       a[2] * (a[3] * a[7] - a[4] * a[6]));
+    double uinv[9];
+    mat3_inverse(c->uvec, uinv);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double s = 0;
+            for (int k = 0; k < 3; ++k) s += uinv[3 * k + i] * uinv[3 * k + j];
+            c->lapcT[3 * i + j] = s;
+        }
+    const int ni[3] = {c->bc[0] == LYNX_BC_PERIODIC ? c->nx : c->nx - 1,
+                       c->bc[1] == LYNX_BC_PERIODIC ? c->ny : c->ny - 1,
+                       c->bc[2] == LYNX_BC_PERIODIC ? c->nz : c->nz - 1};
+    c->dx = c->L[0] / ni[0];
+    c->dy = c->L[1] / ni[1];
+    c->dz = c->L[2] / ni[2];
+    c->dV = c->jac / ((double)ni[0] * ni[1] * ni[2]);
+    const double ix = 1.0 / c->dx, iy = 1.0 / c->dy, iz = 1.0 / c->dz;
+    c->D1x.resize(n);
+    c->D1y.resize(n);
+    c->D1z.resize(n);
+    c->D2x.resize(n);
+    c->D2y.resize(n);
+    c->D2z.resize(n);
+    c->D2xy.assign(n, 0.0);
+    c->D2xz.assign(n, 0.0);
+    c->D2yz.assign(n, 0.0);
+    const double gx = c->orth ? 1.0 : c->lapcT[0], gy = c->orth ? 1.0 : c->lapcT[4],
+                 gz = c->orth ? 1.0 : c->lapcT[8];
+    for (int p = 0; p < n; ++p) {
+        c->D1x[p] = c->w1[p] * ix;
+        c->D1y[p] = c->w1[p] * iy;
+        c->D1z[p] = c->w1[p] * iz;
+        c->D2x[p] = gx * c->w2[p] * ix * ix;
+        c->D2y[p] = gy * c->w2[p] * iy * iy;
+        c->D2z[p] = gz * c->w2[p] * iz * iz;
+        if (!c->orth) {
+            c->D2xy[p] = 2.0 * c->lapcT[1] * c->w1[p] * ix;
+            c->D2xz[p] = 2.0 * c->lapcT[2] * c->w1[p] * ix;
+            c->D2yz[p] = 2.0 * c->lapcT[5] * c->w1[p] * iy;
+        }
+    }
+    if (c->orth) {
+        const double PI = 3.14159265358979323846;
+        const double sx = (c->nx - c->nx % 2) / (double)c->nx, sy = (c->ny - c->ny % 2) / (double)c->ny,
+                     sz = (c->nz - c->nz % 2) / (double)c->nz;
+        double m = c->D2x[0] + c->D2y[0] + c->D2z[0];
+        for (int p = 1; p <= c->R; ++p)
+            m += 2.0 * (c->D2x[p] * std::cos(PI * p * sx) + c->D2y[p] * std::cos(PI * p * sy) +
+                        c->D2z[p] * std::cos(PI * p * sz));
+        c->maxeig = -0.5 * m;
+    } else {
+        double m = std::fabs(c->D2x[0]) + std::fabs(c->D2y[0]) + std::fabs(c->D2z[0]);
+        for (int p = 1; p <= c->R; ++p) {
+            m += 2.0 * (std::fabs(c->D2x[p]) + std::fabs(c->D2y[p]) + std::fabs(c->D2z[p]));
+            m += 2.0 * (std::fabs(c->D2xy[p]) + std::fabs(c->D2xz[p]) + std::fabs(c->D2yz[p]));
+        }
+        c->maxeig = 0.5 * m;
+    }
+}
+
+StencilGeom geom(const lynx_ctx* c) {
+    StencilGeom g;
+    g.nx = c->nx;
+    g.ny = c->ny;
+    g.nz = c->nz;
+    g.R = c->R;
+    g.D2x = c->D2x.data();
+    g.D2y = c->D2y.data();
+    g.D2z = c->D2z.data();
+    return g;
+}
+
+// Ghost multipliers: 1 for periodic, 0 for Dirichlet; Bloch phases for complex data.
+template <typename T> void ghost_phases(const lynx_ctx* c, bool use_k, T* phl, T* phr);
+template <> void ghost_phases<double>(const lynx_ctx* c, bool, double* phl, double* phr) {
+    for (int d = 0; d < 3; ++d) phl[d] = phr[d] = (c->bc[d] == LYNX_BC_PERIODIC) ? 1.0 : 0.0;
+}
+template <> void ghost_phases<float>(const lynx_ctx* c, bool, float* phl, float* phr) {
+    for (int d = 0; d < 3; ++d) phl[d] = phr[d] = (c->bc[d] == LYNX_BC_PERIODIC) ? 1.0f : 0.0f;
+}
+template <> void ghost_phases<double2>(const lynx_ctx* c, bool use_k, double2* phl, double2* phr) {
+    for (int d = 0; d < 3; ++d) {
+        if (c->bc[d] != LYNX_BC_PERIODIC) {
+            phl[d] = phr[d] = make_double2(0, 0);
+            continue;
+        }
+        const double th = use_k ? c->kpt[d] * c->L[d] : 0.0;
+        phl[d] = make_double2(std::cos(th), -std::sin(th));
+        phr[d] = make_double2(std::cos(th), std::sin(th));
+    }
+}
+template <> void ghost_phases<float2>(const lynx_ctx* c, bool use_k, float2* phl, float2* phr) {
+    double2 l[3], r[3];
+    ghost_phases<double2>(c, use_k, l, r);
+    for (int d = 0; d < 3; ++d) {
+        phl[d] = make_float2((float)l[d].x, (float)l[d].y);
+        phr[d] = make_float2((float)r[d].x, (float)r[d].y);
+    }
+}
+
+int update_nl_phases(lynx_ctx* c) {
+    if (!c->has_nl || c->nl.n_img == 0) return LYNX_OK;
+    std::vector<double> ph(2 * c->nl.n_img);
+    for (int i = 0; i < c->nl.n_img; ++i) {
+        const double th = -(c->kpt[0] * c->img_shift[3 * i] + c->kpt[1] * c->img_shift[3 * i + 1] +
+                            c->kpt[2] * c->img_shift[3 * i + 2]);
+        ph[2 * i] = std::cos(th);
+        ph[2 * i + 1] = std::sin(th);
+    }
+    LYNX_CUDA_TRY(cudaMemcpyAsync(c->nl.img_phase, ph.data(), ph.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                  c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return LYNX_OK;
+}
+
+template <typename T> struct Real;
+template <> struct Real<double> { using type = double; };
+template <> struct Real<float> { using type = float; };
+template <> struct Real<double2> { using type = double; };
+template <> struct Real<float2> { using type = float; };
+
+// V (FP64 device) in the scalar type of T.
+template <typename S> const S* veff_as(lynx_ctx* c, const double* v, int* st);
+template <> const double* veff_as<double>(lynx_ctx*, const double* v, int* st) {
+    *st = LYNX_OK;
+    return v;
+}
+template <> const float* veff_as<float>(lynx_ctx* c, const double* v, int* st) {
+    *st = c->v32.ensure(sizeof(float) * c->Nd);
+    if (*st) return nullptr;
+    *st = convert_cols<float, double>(c->v32.as<float>(), c->Nd, v, c->Nd, c->Nd, 1, c->stream);
+    return c->v32.as<float>();
+}
+
+// One fused step: out = a*(H_loc x) + b*x + d*xold, plus the nonlocal part a*Vnl x.
+template <typename T>
+int cheb_step(lynx_ctx* c, const T* x, long long ldx, const T* xold, long long ldo, T* out, long long ldout,
+              const typename Real<T>::type* V, int ncol, double a, double b, double d, bool use_k) {
+    using S = typename Real<T>::type;
+    T phl[3], phr[3];
+    ghost_phases<T>(c, use_k, phl, phr);
+    const int ncolp = ((ncol + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
+    if (c->has_nl) {
+        LYNX_TRY(c->alpha.ensure(sizeof(T) * (size_t)c->nl.total_proj * ncolp));
+        LYNX_TRY(launch_nl_gather<T>(c->nl, x, ldx, ncol, c->alpha.as<T>(), ncolp, c->dV, c->stream));
+    }
+    LYNX_TRY(launch_cheb_step<T, S>(geom(c), x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, c->stream));
+    if (c->has_nl)
+        LYNX_TRY(launch_nl_scatter<T, S>(c->nl, out, ldout, ncol, c->alpha.as<T>(), ncolp, (S)a, c->stream));
+    return LYNX_OK;
+}
+
+// Chebyshev filter (src/solvers/EigenSolver.cpp:559-619) on blocks of type T.
+// X is read at the first two steps only; bufs[0..2] rotate.  Returns the block
+// holding the filtered Y in *yout.
+template <typename T>
+int filter_blocks(lynx_ctx* c, const T* X, long long ldX, T* bufs[3], const typename Real<T>::type* V, int ncol,
+                  double lc, double emin, double emax, int degree, bool use_k, T** yout) {
+    const long long ld = c->Nd;
+    const double e = (emax - lc) / 2.0;
+    const double cc = (emax + lc) / 2.0;
+    const double sigma1 = e / (emin - cc);
+    double sigma = sigma1;
+    // Y = (sigma1/e) (H X - c X)
+    const double s0 = sigma1 / e;
+    LYNX_TRY(cheb_step<T>(c, X, ldX, nullptr, 0, bufs[0], ld, V, ncol, s0, -cc * s0, 0.0, use_k));
+    const T* xold = X;
+    long long ldold = ldX;
+    int iy = 0;
+    for (int k = 2; k <= degree; ++k) {
+        const double sigma_new = 1.0 / (2.0 / sigma1 - sigma);
+        const double gamma = 2.0 * sigma_new / e;
+        const int inew = (iy + 1) % 3;
+        LYNX_TRY(cheb_step<T>(c, bufs[iy], ld, xold, ldold, bufs[inew], ld, V, ncol, gamma, -gamma * cc,
+                              -sigma * sigma_new, use_k));
+        xold = bufs[iy];
+        ldold = ld;
+        iy = inew;
+        sigma = sigma_new;
+    }
+    *yout = bufs[iy];
+    return LYNX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Rayleigh-Ritz in FP64 (cuBLAS / cuSOLVER), real and complex.
+// ---------------------------------------------------------------------------
+#define CUBLAS_TRY(expr)                                                  \
+    do {                                                                  \
+        cublasStatus_t _s = (expr);                                       \
+        if (_s != CUBLAS_STATUS_SUCCESS) {                                \
+            set_error("%s failed: cublas status %d", #expr, (int)_s);    \
+            return LYNX_ERR_CUDA;                                         \
+        }                                                                 \
+    } while (0)
+#define CUSOLVER_TRY(expr)                                                \
+    do {                                                                  \
+        cusolverStatus_t _s = (expr);                                     \
+        if (_s != CUSOLVER_STATUS_SUCCESS) {                              \
+            set_error("%s failed: cusolver status %d", #expr, (int)_s);  \
+            return LYNX_ERR_CUDA;                                         \
+        }                                                                 \
+    } while (0)
+
+int finish_rr(lynx_ctx* c, int N, double* eig_host) {
+    int info[2] = {0, 0};
+    LYNX_CUDA_TRY(cudaMemcpyAsync(info, c->info.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(eig_host, c->eigd.p, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (info[0] != 0) {
+        set_error("Cholesky factorization of the overlap failed (info=%d)", info[0]);
+        return info[0] > 0 ? LYNX_ERR_CHOL_FAIL : LYNX_ERR_BAD_ARG;
+    }
+    if (info[1] != 0) {
+        set_error("subspace eigensolver failed (info=%d, N=%d)", info[1], N);
+        return info[1] > 0 ? LYNX_ERR_EIG_FAIL : LYNX_ERR_BAD_ARG;
+    }
+    for (int i = 0; i < N; ++i)
+        if (!std::isfinite(eig_host[i])) {
+            set_error("non-finite Ritz value at index %d", i);
+            return LYNX_ERR_NONFINITE;
+        }
+    return LYNX_OK;
+}
+
+// psi_out = Y R^-1 Q, eig = eig(R^-T (dV Y^T HY) R^-1), R^T R = dV Y^T Y.
+int rayleigh_ritz_real(lynx_ctx* c, const double* Y, long long ldY, const double* HY, long long ldH,
+                       double* psi, long long ldp, int N, double* eig_host) {
+    const size_t nn = (size_t)N * N;
+    LYNX_TRY(c->Ms.ensure(nn * sizeof(double)));
+    LYNX_TRY(c->Hs.ensure(nn * sizeof(double)));
+    LYNX_TRY(c->eigd.ensure(N * sizeof(double)));
+    LYNX_TRY(c->info.ensure(2 * sizeof(int)));
+    double* Ms = c->Ms.as<double>();
+    double* Hs = c->Hs.as<double>();
+    const double dV = c->dV, one = 1.0, zero = 0.0;
+    CUBLAS_TRY(cublasSetStream(c->cublas, c->stream));
+    CUSOLVER_TRY(cusolverDnSetStream(c->cusolver, c->stream));
+    CUBLAS_TRY(cublasDsyrk(c->cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, N, c->Nd, &dV, Y, ldY, &zero, Ms, N));
+    CUBLAS_TRY(cublasDgemm(c->cublas, CUBLAS_OP_T, CUBLAS_OP_N, N, N, c->Nd, &dV, Y, ldY, HY, ldH, &zero, Hs, N));
+    {
+        dim3 b(16, 16), g((N + 15) / 16, (N + 15) / 16);
+        symmetrize_kernel<<<g, b, 0, c->stream>>>(Hs, N);
+        count_launch();
+    }
+    int lw1 = 0, lw2 = 0;
+    CUSOLVER_TRY(cusolverDnDpotrf_bufferSize(c->cusolver, CUBLAS_FILL_MODE_UPPER, N, Ms, N, &lw1));
+    CUSOLVER_TRY(cusolverDnDsyevd_bufferSize(c->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, N, Hs,
+                                             N, c->eigd.as<double>(), &lw2));
+    const int lw = std::max(lw1, lw2);
+    LYNX_TRY(c->solver_work.ensure((size_t)lw * sizeof(double)));
+    int* info = c->info.as<int>();
+    LYNX_CUDA_TRY(cudaMemsetAsync(info, 0, 2 * sizeof(int), c->stream));
+    CUSOLVER_TRY(cusolverDnDpotrf(c->cusolver, CUBLAS_FILL_MODE_UPPER, N, Ms, N, c->solver_work.as<double>(), lw,
+                                  info));
+    CUBLAS_TRY(cublasDtrsm(c->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
+                           N, N, &one, Ms, N, Hs, N));
+    CUBLAS_TRY(cublasDtrsm(c->cublas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                           N, N, &one, Ms, N, Hs, N));
+    CUSOLVER_TRY(cusolverDnDsyevd(c->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, N, Hs, N,
+                                  c->eigd.as<double>(), c->solver_work.as<double>(), lw, info + 1));
+    CUBLAS_TRY(cublasDtrsm(c->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                           N, N, &one, Ms, N, Hs, N));
+    CUBLAS_TRY(cublasDgemm(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, c->Nd, N, N, &one, Y, ldY, Hs, N, &zero, psi, ldp));
+    return finish_rr(c, N, eig_host);
+}
+
+int rayleigh_ritz_cplx(lynx_ctx* c, const double2* Y, long long ldY, const double2* HY, long long ldH,
+                       double2* psi, long long ldp, int N, double* eig_host) {
+    const size_t nn = (size_t)N * N;
+    LYNX_TRY(c->Ms.ensure(nn * sizeof(double2)));
+    LYNX_TRY(c->Hs.ensure(nn * sizeof(double2)));
+    LYNX_TRY(c->eigd.ensure(N * sizeof(double)));
+    LYNX_TRY(c->info.ensure(2 * sizeof(int)));
+    cuDoubleComplex* Ms = c->Ms.as<cuDoubleComplex>();
+    cuDoubleComplex* Hs = c->Hs.as<cuDoubleComplex>();
+    const cuDoubleComplex* Yz = reinterpret_cast<const cuDoubleComplex*>(Y);
+    const cuDoubleComplex* HYz = reinterpret_cast<const cuDoubleComplex*>(HY);
+    const double dV = c->dV, zero_r = 0.0;
+    const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0),
+                          dVz = make_cuDoubleComplex(dV, 0);
+    CUBLAS_TRY(cublasSetStream(c->cublas, c->stream));
+    CUSOLVER_TRY(cusolverDnSetStream(c->cusolver, c->stream));
+    CUBLAS_TRY(cublasZherk(c->cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, N, c->Nd, &dV, Yz, ldY, &zero_r, Ms, N));
+    CUBLAS_TRY(cublasZgemm(c->cublas, CUBLAS_OP_C, CUBLAS_OP_N, N, N, c->Nd, &dVz, Yz, ldY, HYz, ldH, &zero, Hs, N));
+    {
+        dim3 b(16, 16), g((N + 15) / 16, (N + 15) / 16);
+        hermitize_kernel<<<g, b, 0, c->stream>>>(reinterpret_cast<double2*>(Hs), N);
+        count_launch();
+    }
+    int lw1 = 0, lw2 = 0;
+    CUSOLVER_TRY(cusolverDnZpotrf_bufferSize(c->cusolver, CUBLAS_FILL_MODE_UPPER, N, Ms, N, &lw1));
+    CUSOLVER_TRY(cusolverDnZheevd_bufferSize(c->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, N, Hs,
+                                             N, c->eigd.as<double>(), &lw2));
+    const int lw = std::max(lw1, lw2);
+    LYNX_TRY(c->solver_work.ensure((size_t)lw * sizeof(cuDoubleComplex)));
+    int* info = c->info.as<int>();
+    cuDoubleComplex* work = c->solver_work.as<cuDoubleComplex>();
+    LYNX_CUDA_TRY(cudaMemsetAsync(info, 0, 2 * sizeof(int), c->stream));
+    CUSOLVER_TRY(cusolverDnZpotrf(c->cusolver, CUBLAS_FILL_MODE_UPPER, N, Ms, N, work, lw, info));
+    CUBLAS_TRY(cublasZtrsm(c->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT,
+                           N, N, &one, Ms, N, Hs, N));
+    CUBLAS_TRY(cublasZtrsm(c->cublas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                           N, N, &one, Ms, N, Hs, N));
+    CUSOLVER_TRY(cusolverDnZheevd(c->cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, N, Hs, N,
+                                  c->eigd.as<double>(), work, lw, info + 1));
+    CUBLAS_TRY(cublasZtrsm(c->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
+                           N, N, &one, Ms, N, Hs, N));
+    CUBLAS_TRY(cublasZgemm(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, c->Nd, N, N, &one, Yz, ldY, Hs, N, &zero,
+                           reinterpret_cast<cuDoubleComplex*>(psi), ldp));
+    return finish_rr(c, N, eig_host);
+}
+
+int rayleigh_ritz(lynx_ctx* c, const double* Y, long long ldY, const double* HY, long long ldH, double* psi,
+                  long long ldp, int N, double* eig) {
+    return rayleigh_ritz_real(c, Y, ldY, HY, ldH, psi, ldp, N, eig);
+}
+int rayleigh_ritz(lynx_ctx* c, const double2* Y, long long ldY, const double2* HY, long long ldH, double2* psi,
+                  long long ldp, int N, double* eig) {
+    return rayleigh_ritz_cplx(c, Y, ldY, HY, ldH, psi, ldp, N, eig);
+}
+
+// ---------------------------------------------------------------------------
+// CheFSI pass.  T64 = FP64 storage type (double / double2), T32 = FP32 (float / float2).
+// ---------------------------------------------------------------------------
+template <typename T64, typename T32>
+int solve_impl(lynx_ctx* c, T64* psi, double* eig, const double* veff, int N, int ld, double lc, double emin,
+               double emax, int degree, int precision, double* lc_out, bool use_k) {
+    LYNX_CHECK_ARG(c != nullptr, "null context");
+    LYNX_CHECK_ARG(psi != nullptr && eig != nullptr && veff != nullptr, "null pointer");
+    LYNX_CHECK_ARG(N > 0, "nband must be positive");
+    LYNX_CHECK_ARG(degree >= 1, "cheb_degree must be >= 1");
+    LYNX_CHECK_ARG(precision == LYNX_PREC_FP64 || precision == LYNX_PREC_MIXED, "unknown precision");
+    LYNX_CHECK_ARG(emax > lc && emin < lc, "spectral bounds must satisfy eigmin < lambda_cutoff < eigmax");
+    if (!c->orth) {
+        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    LYNX_TRY(activate(c));
+    const long long Nd = c->Nd;
+    const long long ldp = ld > 0 ? ld : Nd;
+    LYNX_CHECK_ARG(ldp >= Nd, "ld < Nd");
+    if (precision == LYNX_PREC_FP64) {
+        const size_t blk = sizeof(T64) * (size_t)Nd * N;
+        for (int i = 0; i < 3; ++i) LYNX_TRY(c->wbuf[i].ensure(blk));
+        T64* bufs[3] = {c->wbuf[0].as<T64>(), c->wbuf[1].as<T64>(), c->wbuf[2].as<T64>()};
+        T64* Y = nullptr;
+        LYNX_TRY(filter_blocks<T64>(c, psi, ldp, bufs, veff, N, lc, emin, emax, degree, use_k, &Y));
+        T64* HY = (Y == bufs[0]) ? bufs[1] : bufs[0];
+        LYNX_TRY(cheb_step<T64>(c, Y, Nd, nullptr, 0, HY, Nd, veff, N, 1.0, 0.0, 0.0, use_k));
+        LYNX_TRY(rayleigh_ritz(c, Y, Nd, HY, Nd, psi, ldp, N, eig));
+    } else {
+        int st = LYNX_OK;
+        const float* v32 = veff_as<float>(c, veff, &st);
+        if (st) return st;
+        const size_t blk = sizeof(T32) * (size_t)Nd * N;
+        for (int i = 0; i < 4; ++i) LYNX_TRY(c->wbuf[i].ensure(blk));
+        T32* X32 = c->wbuf[3].as<T32>();
+        LYNX_TRY(convert_cols<T32, T64>(X32, Nd, psi, ldp, Nd, N, c->stream));
+        T32* bufs[3] = {c->wbuf[0].as<T32>(), c->wbuf[1].as<T32>(), c->wbuf[2].as<T32>()};
+        T32* Y = nullptr;
+        LYNX_TRY(filter_blocks<T32>(c, X32, Nd, bufs, v32, N, lc, emin, emax, degree, use_k, &Y));
+        T32* HY = (Y == bufs[0]) ? bufs[1] : bufs[0];
+        LYNX_TRY(cheb_step<T32>(c, Y, Nd, nullptr, 0, HY, Nd, v32, N, 1.0, 0.0, 0.0, use_k));
+        // Rayleigh-Ritz products on FP64 copies of the FP32 blocks.
+        const size_t blk64 = sizeof(T64) * (size_t)Nd * N;
+        LYNX_TRY(c->cvt[0].ensure(blk64));
+        LYNX_TRY(c->cvt[1].ensure(blk64));
+        LYNX_TRY(convert_cols<T64, T32>(c->cvt[0].as<T64>(), Nd, Y, Nd, Nd, N, c->stream));
+        LYNX_TRY(convert_cols<T64, T32>(c->cvt[1].as<T64>(), Nd, HY, Nd, Nd, N, c->stream));
+        LYNX_TRY(rayleigh_ritz(c, c->cvt[0].as<T64>(), Nd, c->cvt[1].as<T64>(), Nd, psi, ldp, N, eig));
+    }
+    if (lc_out) *lc_out = eig[N - 1] + 0.1;
+    return LYNX_OK;
+}
+
+// Bisection count of eigenvalues of the symmetric tridiagonal (d, e) below x (Sturm sequence).
+int sturm_count(const std::vector<double>& d, const std::vector<double>& e, int n, double x) {
+    int cnt = 0;
+    double q = 1.0;
+    for (int i = 0; i < n; ++i) {
+        const double off = (i > 0) ? e[i - 1] * e[i - 1] : 0.0;
+        q = d[i] - x - (i > 0 ? off / q : 0.0);
+        if (q == 0.0) q = -1e-300;
+        if (q < 0) ++cnt;
+    }
+    return cnt;
+}
+
+// Smallest and largest eigenvalue of an n x n symmetric tridiagonal matrix by bisection.
+void tridiag_extremes(const std::vector<double>& d, const std::vector<double>& e, int n, double* lo,
+                      double* hi) {
+    double gl = d[0], gu = d[0];
+    for (int i = 0; i < n; ++i) {
+        const double r = (i > 0 ? std::fabs(e[i - 1]) : 0.0) + (i < n - 1 ? std::fabs(e[i]) : 0.0);
+        gl = std::min(gl, d[i] - r);
+        gu = std::max(gu, d[i] + r);
+    }
+    const double span = std::max(std::fabs(gl), std::fabs(gu));
+    auto bisect = [&](int k) {  // k-th smallest (0-based)
+        double a = gl - 1e-12 * span - 1e-300, b = gu + 1e-12 * span + 1e-300;
+        for (int it = 0; it < 200; ++it) {
+            const double m = 0.5 * (a + b);
+            if (m == a || m == b) break;
+            if (sturm_count(d, e, n, m) > k) b = m;
+            else a = m;
+        }
+        return 0.5 * (a + b);
+    };
+    *lo = bisect(0);
+    *hi = bisect(n - 1);
+}
+
+template <typename T>
+__global__ void lanczos_update_kernel(T* __restrict__ vp1, T* __restrict__ vj, T* __restrict__ vjm1, double a,
+                                      double b, long long n) {
+    // vp1 -= a*vj + b*vjm1; vjm1 = vj
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        vp1[i] = vp1[i] - a * vj[i] - b * vjm1[i];
+        vjm1[i] = vj[i];
+    }
+}
+
+// Lanczos extreme-eigenvalue estimate (src/solvers/Lanczos.hpp:92-200), vectors on the device.
+// Real data: Nv = Nd doubles; complex: Nv = 2*Nd doubles viewed as interleaved complex.
+template <typename T>
+int lanczos_impl(lynx_ctx* c, const double* veff, double tol, int max_iter, double* eigmin, double* eigmax,
+                 bool use_k) {
+    LYNX_CHECK_ARG(c && veff && eigmin && eigmax, "null pointer");
+    LYNX_CHECK_ARG(max_iter >= 1, "max_iter must be >= 1");
+    if (!c->orth) {
+        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    LYNX_TRY(activate(c));
+    const bool cplx = sizeof(T) == sizeof(double2);
+    const long long Nv = cplx ? 2LL * c->Nd : c->Nd;  // doubles per vector
+    for (int i = 0; i < 3; ++i) LYNX_TRY(c->lz[i].ensure(Nv * sizeof(double)));
+    double* vjm1 = c->lz[0].as<double>();
+    double* vj = c->lz[1].as<double>();
+    double* vp1 = c->lz[2].as<double>();
+    // Start vector: srand(1); entries rand()/RAND_MAX (re, im interleaved for complex).
+    std::vector<double> h(Nv);
+    std::srand(1);
+    for (long long i = 0; i < Nv; ++i) h[i] = (double)std::rand() / RAND_MAX;
+    double nrm = 0;
+    for (double v : h) nrm += v * v;
+    const double sc = 1.0 / std::sqrt(nrm);
+    for (double& v : h) v *= sc;
+    LYNX_CUDA_TRY(cudaMemcpyAsync(vjm1, h.data(), Nv * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CUBLAS_TRY(cublasSetStream(c->cublas, c->stream));
+    auto Happly = [&](const double* x, double* y) -> int {
+        return cheb_step<T>(c, reinterpret_cast<const T*>(x), c->Nd, nullptr, 0, reinterpret_cast<T*>(y), c->Nd,
+                            veff, 1, 1.0, 0.0, 0.0, use_k);
+    };
+    auto dot = [&](const double* x, const double* y, double* r) -> int {
+        CUBLAS_TRY(cublasDdot(c->cublas, (int)Nv, x, 1, y, 1, r));  // Re<x,y> for interleaved complex too
+        return LYNX_OK;
+    };
+    auto norm = [&](const double* x, double* r) -> int {
+        CUBLAS_TRY(cublasDnrm2(c->cublas, (int)Nv, x, 1, r));
+        return LYNX_OK;
+    };
+    std::vector<double> a(max_iter + 1, 0.0), b(max_iter + 1, 0.0);
+    LYNX_TRY(Happly(vjm1, vj));
+    LYNX_TRY(dot(vjm1, vj, &a[0]));
+    {
+        const double m = -a[0];
+        CUBLAS_TRY(cublasDaxpy(c->cublas, (int)Nv, &m, vjm1, 1, vj, 1));
+    }
+    LYNX_TRY(norm(vj, &b[0]));
+    if (b[0] == 0.0) {
+        set_error("Lanczos start vector spans an invariant subspace");
+        return LYNX_ERR_NONFINITE;
+    }
+    {
+        const double s = 1.0 / b[0];
+        CUBLAS_TRY(cublasDscal(c->cublas, (int)Nv, &s, vj, 1));
+    }
+    double emin = 0, emax = 0, pmin = 0, pmax = 0, errmin = tol + 1, errmax = tol + 1;
+    int j = 0;
+    std::vector<double> d, e;
+    const int blocks = (int)std::min<long long>((Nv + 255) / 256, 148 * 8);
+    while ((errmin > tol || errmax > tol) && j < max_iter) {
+        LYNX_TRY(Happly(vj, vp1));
+        LYNX_TRY(dot(vj, vp1, &a[j + 1]));
+        lanczos_update_kernel<double><<<blocks, 256, 0, c->stream>>>(vp1, vj, vjm1, a[j + 1], b[j], Nv);
+        count_launch();
+        LYNX_TRY(norm(vp1, &b[j + 1]));
+        if (b[j + 1] == 0.0) break;
+        const double s = 1.0 / b[j + 1];
+        LYNX_CUDA_TRY(cudaMemcpyAsync(vj, vp1, Nv * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        CUBLAS_TRY(cublasDscal(c->cublas, (int)Nv, &s, vj, 1));
+        const int n = j + 2;
+        d.assign(a.begin(), a.begin() + n);
+        e.assign(b.begin(), b.begin() + n);
+        tridiag_extremes(d, e, n, &emin, &emax);
+        errmin = std::fabs(emin - pmin);
+        errmax = std::fabs(emax - pmax);
+        pmin = emin;
+        pmax = emax;
+        ++j;
+    }
+    *eigmax = emax * 1.01;
+    *eigmin = emin - 0.1;
+    return LYNX_OK;
+}
+
+// Brent's root finder (R. P. Brent, Algorithms for Minimization Without Derivatives, 1973, ch. 4)
+// for f(a) f(b) <= 0, absolute tolerance tol.
+template <typename F>
+double brent_zero(F f, double a, double b, double tol, int max_iter) {
+    double fa = f(a), fb = f(b);
+    double c = a, fc = fa, d = b - a, e = d;
+    for (int it = 0; it < max_iter; ++it) {
+        if ((fb > 0 && fc > 0) || (fb < 0 && fc < 0)) {
+            c = a;
+            fc = fa;
+            d = e = b - a;
+        }
+        if (std::fabs(fc) < std::fabs(fb)) {
+            a = b;
+            b = c;
+            c = a;
+            fa = fb;
+            fb = fc;
+            fc = fa;
+        }
+        const double tol1 = 2.0 * std::numeric_limits<double>::epsilon() * std::fabs(b) + 0.5 * tol;
+        const double m = 0.5 * (c - b);
+        if (std::fabs(m) <= tol1 || fb == 0.0) return b;
+        if (std::fabs(e) >= tol1 && std::fabs(fa) > std::fabs(fb)) {
+            // inverse quadratic interpolation, or secant when only two points differ
+            const double s = fb / fa;
+            double p, q;
+            if (a == c) {
+                p = 2.0 * m * s;
+                q = 1.0 - s;
+            } else {
+                const double qa = fa / fc, r = fb / fc;
+                p = s * (2.0 * m * qa * (qa - r) - (b - a) * (r - 1.0));
+                q = (qa - 1.0) * (r - 1.0) * (s - 1.0);
+            }
+            if (p > 0) q = -q;
+            else p = -p;
+            if (2.0 * p < std::min(3.0 * m * q - std::fabs(tol1 * q), std::fabs(e * q))) {
+                e = d;
+                d = p / q;
+            } else {
+                d = m;
+                e = d;
+            }
+        } else {
+            d = m;
+            e = d;
+        }
+        a = b;
+        fa = fb;
+        b += (std::fabs(d) > tol1) ? d : (m > 0 ? tol1 : -tol1);
+        fb = f(b);
+    }
+    return b;
+}
+
+double smear(double x, double beta, int type) {
+    if (type == LYNX_SMEAR_FERMI_DIRAC) {
+        const double t = x * beta;
+        if (t > 50.0) return 0.0;
+        if (t < -50.0) return 1.0;
+        return 1.0 / (1.0 + std::exp(t));
+    }
+    return 0.5 * std::erfc(beta * x);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Exported C entry points
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* lynx_status_string(int s) {
+    switch (s) {
+        case LYNX_OK: return "ok";
+        case LYNX_ERR_BAD_ARG: return "bad argument";
+        case LYNX_ERR_CUDA: return "CUDA error";
+        case LYNX_ERR_OOM: return "out of device memory";
+        case LYNX_ERR_CHOL_FAIL: return "Cholesky factorization failed";
+        case LYNX_ERR_EIG_FAIL: return "subspace eigensolver failed";
+        case LYNX_ERR_NONFINITE: return "non-finite values";
+        case LYNX_ERR_TIMEOUT: return "device wait timed out";
+        case LYNX_ERR_NOT_SETUP: return "not set up";
+        case LYNX_ERR_UNSUPPORTED: return "unsupported configuration";
+        case LYNX_ERR_BRACKET: return "Fermi level cannot be bracketed";
+        default: return "unknown status";
+    }
+}
+
+const char* lynx_last_error(void) { return g_last_error.c_str(); }
+int lynx_version(void) { return 1; }
+long long lynx_launch_count(int reset) {
+    return reset ? g_launches.exchange(0) : g_launches.load();
+}
+
+int lynx_create(lynx_ctx** out, int device, int nx, int ny, int nz, int fd_order, const double* latvec,
+                int orthogonal, const int* bc) {
+    LYNX_CHECK_ARG(out != nullptr && latvec != nullptr, "null pointer");
+    *out = nullptr;
+    LYNX_CHECK_ARG(nx > 0 && ny > 0 && nz > 0, "grid dimensions must be positive");
+    LYNX_CHECK_ARG(fd_order >= 2 && fd_order % 2 == 0, "FD order must be even and >= 2");
+    lynx_ctx* c = new lynx_ctx();
+    c->device = device;
+    c->nx = nx;
+    c->ny = ny;
+    c->nz = nz;
+    c->Nd = nx * ny * nz;
+    c->fd_order = fd_order;
+    c->R = fd_order / 2;
+    c->orth = orthogonal != 0;
+    for (int d = 0; d < 3; ++d) c->bc[d] = bc ? bc[d] : LYNX_BC_PERIODIC;
+    std::memcpy(c->latvec, latvec, 9 * sizeof(double));
+    build_stencil(c);
+    if (!(c->jac > 1e-14)) {
+        delete c;
+        set_error("lattice vectors are coplanar");
+        return LYNX_ERR_BAD_ARG;
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        delete c;
+        set_error("cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+        return LYNX_ERR_CUDA;
+    }
+    if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS || cusolverDnCreate(&c->cusolver) != CUSOLVER_STATUS_SUCCESS) {
+        if (c->cublas) cublasDestroy(c->cublas);
+        delete c;
+        set_error("cuBLAS/cuSOLVER initialisation failed");
+        return LYNX_ERR_CUDA;
+    }
+    *out = c;
+    return LYNX_OK;
+}
+
+int lynx_destroy(lynx_ctx* c) {
+    if (!c) return LYNX_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    else cudaDeviceSynchronize();
+    for (auto& b : c->wbuf) b.release();
+    for (auto& b : c->cvt) b.release();
+    for (auto& b : c->lz) b.release();
+    for (auto& b : c->nl_bufs) b.release();
+    c->alpha.release();
+    c->v32.release();
+    c->Ms.release();
+    c->Hs.release();
+    c->eigd.release();
+    c->solver_work.release();
+    c->info.release();
+    c->io_psi.release();
+    c->io_v.release();
+    if (c->cublas) cublasDestroy(c->cublas);
+    if (c->cusolver) cusolverDnDestroy(c->cusolver);
+    delete c;
+    return LYNX_OK;
+}
+
+int lynx_set_stream(lynx_ctx* c, void* stream) {
+    LYNX_CHECK_ARG(c != nullptr, "null context");
+    c->stream = static_cast<cudaStream_t>(stream);
+    return LYNX_OK;
+}
+
+int lynx_grid_info(const lynx_ctx* c, int* nd, double* dV, double* maxeig) {
+    LYNX_CHECK_ARG(c != nullptr, "null context");
+    if (nd) *nd = c->Nd;
+    if (dV) *dV = c->dV;
+    if (maxeig) *maxeig = c->maxeig;
+    return LYNX_OK;
+}
+
+int lynx_stencil_coeffs(const lynx_ctx* c, double* d2x, double* d2y, double* d2z, double* d2xy, double* d2xz,
+                        double* d2yz, double* d1x, double* d1y, double* d1z) {
+    LYNX_CHECK_ARG(c != nullptr, "null context");
+    auto cp = [&](double* dst, const std::vector<double>& v) {
+        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(double));
+    };
+    cp(d2x, c->D2x);
+    cp(d2y, c->D2y);
+    cp(d2z, c->D2z);
+    cp(d2xy, c->D2xy);
+    cp(d2xz, c->D2xz);
+    cp(d2yz, c->D2yz);
+    cp(d1x, c->D1x);
+    cp(d1y, c->D1y);
+    cp(d1z, c->D1z);
+    return LYNX_OK;
+}
+
+int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* img_ndc, const double* img_shift,
+                      const int* gpos, const double* chi, int n_atom, const int* atom_nproj, const double* gamma) {
+    LYNX_CHECK_ARG(c != nullptr, "null context");
+    LYNX_TRY(activate(c));
+    for (auto& b : c->nl_bufs) b.release();
+    c->nl_bufs.clear();
+    c->nl = NLDev();
+    c->has_nl = false;
+    c->img_shift.clear();
+    if (n_img == 0) return LYNX_OK;
+    LYNX_CHECK_ARG(n_img > 0 && n_atom > 0, "counts must be positive");
+    LYNX_CHECK_ARG(img_atom && img_ndc && img_shift && gpos && chi && atom_nproj && gamma, "null table");
+    // per-atom projector offsets and image lists
+    std::vector<int> poff(n_atom + 1, 0), nproj(atom_nproj, atom_nproj + n_atom);
+    int max_np = 0;
+    for (int a = 0; a < n_atom; ++a) {
+        LYNX_CHECK_ARG(nproj[a] >= 0, "negative projector count");
+        poff[a + 1] = poff[a] + nproj[a];
+        max_np = std::max(max_np, nproj[a]);
+    }
+    std::vector<int> img_ptr(n_atom + 1, 0), img_list(n_img);
+    std::vector<long long> goff(n_img), choff(n_img);
+    long long tot = 0, totchi = 0;
+    for (int i = 0; i < n_img; ++i) {
+        LYNX_CHECK_ARG(img_atom[i] >= 0 && img_atom[i] < n_atom, "image atom index out of range");
+        LYNX_CHECK_ARG(img_ndc[i] >= 0, "negative image point count");
+        goff[i] = tot;
+        choff[i] = totchi;
+        tot += img_ndc[i];
+        totchi += (long long)img_ndc[i] * nproj[img_atom[i]];
+        img_ptr[img_atom[i] + 1]++;
+    }
+    for (int a = 0; a < n_atom; ++a) img_ptr[a + 1] += img_ptr[a];
+    {
+        std::vector<int> fill(img_ptr.begin(), img_ptr.end() - 1);
+        for (int i = 0; i < n_img; ++i) img_list[fill[img_atom[i]]++] = i;  // image order preserved per atom
+    }
+    for (long long k = 0; k < tot; ++k)
+        LYNX_CHECK_ARG(gpos[k] >= 0 && gpos[k] < c->Nd, "grid position out of range");
+    // CSR over distinct grid points, entries in (image, local index) order.
+    std::vector<long long> keys(tot);
+    {
+        long long k = 0;
+        for (int i = 0; i < n_img; ++i)
+            for (int l = 0; l < img_ndc[i]; ++l, ++k) keys[k] = ((long long)gpos[k] << 32) | (unsigned)k;
+    }
+    std::sort(keys.begin(), keys.end());
+    std::vector<int> pt_grid, pt_ptr, ent_img(tot), ent_loc(tot);
+    std::vector<int> owner_img(tot), owner_loc(tot);
+    {
+        long long k = 0;
+        for (int i = 0; i < n_img; ++i)
+            for (int l = 0; l < img_ndc[i]; ++l, ++k) {
+                owner_img[k] = i;
+                owner_loc[k] = l;
+            }
+    }
+    for (long long s = 0; s < tot; ++s) {
+        const int g = (int)(keys[s] >> 32);
+        const long long k = keys[s] & 0xFFFFFFFFLL;
+        if (pt_grid.empty() || pt_grid.back() != g) {
+            pt_grid.push_back(g);
+            pt_ptr.push_back((int)s);
+        }
+        ent_img[s] = owner_img[k];
+        ent_loc[s] = owner_loc[k];
+    }
+    pt_ptr.push_back((int)tot);
+    std::vector<float> chi32(totchi);
+    for (long long k = 0; k < totchi; ++k) chi32[k] = (float)chi[k];
+    // upload
+    auto up = [&](const void* src, size_t bytes, void** dst) -> int {
+        c->nl_bufs.emplace_back();
+        DevBuf& b = c->nl_bufs.back();
+        LYNX_TRY(b.ensure(std::max<size_t>(bytes, 16)));
+        if (bytes) LYNX_CUDA_TRY(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
+        *dst = b.p;
+        return LYNX_OK;
+    };
+    c->nl_bufs.reserve(20);
+    NLDev& d = c->nl;
+    d.n_atom = n_atom;
+    d.n_img = n_img;
+    d.n_pts = (int)pt_grid.size();
+    d.max_np = max_np;
+    d.total_proj = poff[n_atom];
+    LYNX_TRY(up(img_ptr.data(), img_ptr.size() * 4, (void**)&d.atom_img_ptr));
+    LYNX_TRY(up(img_list.data(), img_list.size() * 4, (void**)&d.atom_img_list));
+    LYNX_TRY(up(nproj.data(), nproj.size() * 4, (void**)&d.atom_nproj));
+    LYNX_TRY(up(poff.data(), poff.size() * 4, (void**)&d.atom_poff));
+    LYNX_TRY(up(gamma, (size_t)poff[n_atom] * 8, (void**)&d.gamma));
+    LYNX_TRY(up(img_atom, (size_t)n_img * 4, (void**)&d.img_atom));
+    LYNX_TRY(up(img_ndc, (size_t)n_img * 4, (void**)&d.img_ndc));
+    LYNX_TRY(up(goff.data(), goff.size() * 8, (void**)&d.img_goff));
+    LYNX_TRY(up(choff.data(), choff.size() * 8, (void**)&d.img_chi_off));
+    std::vector<double> ph(2 * n_img, 0.0);
+    for (int i = 0; i < n_img; ++i) ph[2 * i] = 1.0;
+    LYNX_TRY(up(ph.data(), ph.size() * 8, (void**)&d.img_phase));
+    LYNX_TRY(up(gpos, (size_t)tot * 4, (void**)&d.gpos));
+    LYNX_TRY(up(chi, (size_t)totchi * 8, (void**)&d.chi64));
+    LYNX_TRY(up(chi32.data(), (size_t)totchi * 4, (void**)&d.chi32));
+    LYNX_TRY(up(pt_grid.data(), pt_grid.size() * 4, (void**)&d.pt_grid));
+    LYNX_TRY(up(pt_ptr.data(), pt_ptr.size() * 4, (void**)&d.pt_ptr));
+    LYNX_TRY(up(ent_img.data(), ent_img.size() * 4, (void**)&d.ent_img));
+    LYNX_TRY(up(ent_loc.data(), ent_loc.size() * 4, (void**)&d.ent_loc));
+    c->img_shift.assign(img_shift, img_shift + 3 * n_img);
+    c->has_nl = true;
+    return update_nl_phases(c);
+}
+
+int lynx_set_kpoint(lynx_ctx* c, const double* k) {
+    LYNX_CHECK_ARG(c != nullptr && k != nullptr, "null pointer");
+    LYNX_TRY(activate(c));
+    for (int d = 0; d < 3; ++d) c->kpt[d] = k[d];
+    return update_nl_phases(c);
+}
+
+int lynx_hamiltonian_apply(lynx_ctx* c, const double* psi, const double* veff, double* y, int ncol, int ld,
+                           double cs) {
+    LYNX_CHECK_ARG(c && psi && veff && y, "null pointer");
+    LYNX_CHECK_ARG(ncol >= 0, "negative ncol");
+    if (!c->orth) {
+        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    LYNX_TRY(activate(c));
+    const long long l = ld > 0 ? ld : c->Nd;
+    LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
+    return cheb_step<double>(c, psi, l, nullptr, 0, y, l, veff, ncol, 1.0, cs, 0.0, false);
+}
+
+int lynx_hamiltonian_apply_kpt(lynx_ctx* c, const double* psi, const double* veff, double* y, int ncol, int ld,
+                               double cs) {
+    LYNX_CHECK_ARG(c && psi && veff && y, "null pointer");
+    LYNX_CHECK_ARG(ncol >= 0, "negative ncol");
+    if (!c->orth) {
+        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    LYNX_TRY(activate(c));
+    const long long l = ld > 0 ? ld : c->Nd;
+    LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
+    return cheb_step<double2>(c, reinterpret_cast<const double2*>(psi), l, nullptr, 0,
+                              reinterpret_cast<double2*>(y), l, veff, ncol, 1.0, cs, 0.0, true);
+}
+
+int lynx_nonlocal_apply(lynx_ctx* c, const double* psi, double* hpsi, int ncol, int ld) {
+    LYNX_CHECK_ARG(c && psi && hpsi, "null pointer");
+    if (!c->has_nl) return LYNX_OK;
+    LYNX_TRY(activate(c));
+    const long long l = ld > 0 ? ld : c->Nd;
+    const int ncolp = ((ncol + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
+    LYNX_TRY(c->alpha.ensure(sizeof(double) * (size_t)c->nl.total_proj * ncolp));
+    LYNX_TRY(launch_nl_gather<double>(c->nl, psi, l, ncol, c->alpha.as<double>(), ncolp, c->dV, c->stream));
+    return launch_nl_scatter<double, double>(c->nl, hpsi, l, ncol, c->alpha.as<double>(), ncolp, 1.0, c->stream);
+}
+
+int lynx_nonlocal_apply_kpt(lynx_ctx* c, const double* psi, double* hpsi, int ncol, int ld) {
+    LYNX_CHECK_ARG(c && psi && hpsi, "null pointer");
+    if (!c->has_nl) return LYNX_OK;
+    LYNX_TRY(activate(c));
+    const long long l = ld > 0 ? ld : c->Nd;
+    const int ncolp = ((ncol + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
+    LYNX_TRY(c->alpha.ensure(sizeof(double2) * (size_t)c->nl.total_proj * ncolp));
+    LYNX_TRY(launch_nl_gather<double2>(c->nl, reinterpret_cast<const double2*>(psi), l, ncol,
+                                       c->alpha.as<double2>(), ncolp, c->dV, c->stream));
+    return launch_nl_scatter<double2, double>(c->nl, reinterpret_cast<double2*>(hpsi), l, ncol,
+                                              c->alpha.as<double2>(), ncolp, 1.0, c->stream);
+}
+
+static int filter_entry(lynx_ctx* c, const double* X, double* Y, const double* veff, int ncol, int ld, double lc,
+                        double emin, double emax, int degree, int precision, bool cplx) {
+    LYNX_CHECK_ARG(c && X && Y && veff, "null pointer");
+    LYNX_CHECK_ARG(ncol > 0 && degree >= 1, "ncol and degree must be positive");
+    LYNX_CHECK_ARG(precision == LYNX_PREC_FP64 || precision == LYNX_PREC_MIXED, "unknown precision");
+    LYNX_CHECK_ARG(emax > lc && emin < lc, "spectral bounds must satisfy eigmin < lambda_cutoff < eigmax");
+    if (!c->orth) {
+        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    LYNX_TRY(activate(c));
+    const long long Nd = c->Nd, l = ld > 0 ? ld : Nd;
+    LYNX_CHECK_ARG(l >= Nd, "ld < Nd");
+    const size_t esz = cplx ? 2 : 1;
+    if (precision == LYNX_PREC_FP64) {
+        const size_t blk = sizeof(double) * esz * (size_t)Nd * ncol;
+        for (int i = 0; i < 3; ++i) LYNX_TRY(c->wbuf[i].ensure(blk));
+        if (cplx) {
+            double2* b[3] = {c->wbuf[0].as<double2>(), c->wbuf[1].as<double2>(), c->wbuf[2].as<double2>()};
+            double2* out = nullptr;
+            LYNX_TRY(filter_blocks<double2>(c, reinterpret_cast<const double2*>(X), l, b, veff, ncol, lc, emin, emax,
+                                            degree, true, &out));
+            LYNX_CUDA_TRY(cudaMemcpy2DAsync(Y, l * 16, out, Nd * 16, Nd * 16, ncol, cudaMemcpyDeviceToDevice, c->stream));
+        } else {
+            double* b[3] = {c->wbuf[0].as<double>(), c->wbuf[1].as<double>(), c->wbuf[2].as<double>()};
+            double* out = nullptr;
+            LYNX_TRY(filter_blocks<double>(c, X, l, b, veff, ncol, lc, emin, emax, degree, false, &out));
+            LYNX_CUDA_TRY(cudaMemcpy2DAsync(Y, l * 8, out, Nd * 8, Nd * 8, ncol, cudaMemcpyDeviceToDevice, c->stream));
+        }
+    } else {
+        int st = LYNX_OK;
+        const float* v32 = veff_as<float>(c, veff, &st);
+        if (st) return st;
+        const size_t blk = sizeof(float) * esz * (size_t)Nd * ncol;
+        for (int i = 0; i < 4; ++i) LYNX_TRY(c->wbuf[i].ensure(blk));
+        if (cplx) {
+            float2* X32 = c->wbuf[3].as<float2>();
+            LYNX_TRY(convert_cols<float2, double2>(X32, Nd, reinterpret_cast<const double2*>(X), l, Nd, ncol, c->stream));
+            float2* b[3] = {c->wbuf[0].as<float2>(), c->wbuf[1].as<float2>(), c->wbuf[2].as<float2>()};
+            float2* out = nullptr;
+            LYNX_TRY(filter_blocks<float2>(c, X32, Nd, b, v32, ncol, lc, emin, emax, degree, true, &out));
+            LYNX_TRY(convert_cols<double2, float2>(reinterpret_cast<double2*>(Y), l, out, Nd, Nd, ncol, c->stream));
+        } else {
+            float* X32 = c->wbuf[3].as<float>();
+            LYNX_TRY(convert_cols<float, double>(X32, Nd, X, l, Nd, ncol, c->stream));
+            float* b[3] = {c->wbuf[0].as<float>(), c->wbuf[1].as<float>(), c->wbuf[2].as<float>()};
+            float* out = nullptr;
+            LYNX_TRY(filter_blocks<float>(c, X32, Nd, b, v32, ncol, lc, emin, emax, degree, false, &out));
+            LYNX_TRY(convert_cols<double, float>(Y, l, out, Nd, Nd, ncol, c->stream));
+        }
+    }
+    return LYNX_OK;
+}
+
+int lynx_chebyshev_filter(lynx_ctx* c, const double* X, double* Y, const double* veff, int ncol, int ld, double lc,
+                          double emin, double emax, int degree, int precision) {
+    return filter_entry(c, X, Y, veff, ncol, ld, lc, emin, emax, degree, precision, false);
+}
+
+int lynx_chebyshev_filter_kpt(lynx_ctx* c, const double* X, double* Y, const double* veff, int ncol, int ld,
+                              double lc, double emin, double emax, int degree, int precision) {
+    return filter_entry(c, X, Y, veff, ncol, ld, lc, emin, emax, degree, precision, true);
+}
+
+int lynx_eigensolver_solve(lynx_ctx* c, double* psi, double* eig, const double* veff, int nband, int ld, double lc,
+                           double emin, double emax, int degree, int precision, double* lc_out) {
+    return solve_impl<double, float>(c, psi, eig, veff, nband, ld, lc, emin, emax, degree, precision, lc_out, false);
+}
+
+int lynx_eigensolver_solve_kpt(lynx_ctx* c, double* psi, double* eig, const double* veff, int nband, int ld,
+                               double lc, double emin, double emax, int degree, int precision, double* lc_out) {
+    return solve_impl<double2, float2>(c, reinterpret_cast<double2*>(psi), eig, veff, nband, ld, lc, emin, emax,
+                                       degree, precision, lc_out, true);
+}
+
+int lynx_eigensolver_solve_host(lynx_ctx* c, double* psi, double* eig, const double* veff, int nband, int ld,
+                                double lc, double emin, double emax, int degree, int precision, double* lc_out) {
+    LYNX_CHECK_ARG(c && psi && eig && veff, "null pointer");
+    LYNX_CHECK_ARG(nband > 0, "nband must be positive");
+    LYNX_TRY(activate(c));
+    const long long Nd = c->Nd, l = ld > 0 ? ld : Nd;
+    LYNX_CHECK_ARG(l >= Nd, "ld < Nd");
+    DevBuf& dpsi = c->io_psi;
+    DevBuf& dv = c->io_v;
+    LYNX_TRY(dpsi.ensure(sizeof(double) * (size_t)Nd * nband));
+    LYNX_TRY(dv.ensure(sizeof(double) * (size_t)Nd));
+    LYNX_CUDA_TRY(cudaMemcpy2DAsync(dpsi.p, Nd * 8, psi, l * 8, Nd * 8, nband, cudaMemcpyHostToDevice, c->stream));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(dv.p, veff, Nd * 8, cudaMemcpyHostToDevice, c->stream));
+    int st = lynx_eigensolver_solve(c, dpsi.as<double>(), eig, dv.as<double>(), nband, (int)Nd, lc, emin, emax,
+                                    degree, precision, lc_out);
+    if (st == LYNX_OK) {
+        cudaError_t e = cudaMemcpy2DAsync(psi, l * 8, dpsi.p, Nd * 8, Nd * 8, nband, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            set_error("copy-out failed: %s", cudaGetErrorString(e));
+            st = LYNX_ERR_CUDA;
+        }
+    }
+    cudaStreamSynchronize(c->stream);
+    return st;
+}
+
+int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precision, int with_nonlocal, int reps,
+                          double* ms_per_step) {
+    LYNX_CHECK_ARG(c && veff && ms_per_step, "null pointer");
+    LYNX_CHECK_ARG(ncol > 0 && reps > 0, "ncol and reps must be positive");
+    LYNX_CHECK_ARG(precision == LYNX_PREC_FP64 || precision == LYNX_PREC_MIXED, "unknown precision");
+    if (!c->orth) {
+        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    LYNX_TRY(activate(c));
+    const long long Nd = c->Nd;
+    const size_t esz = precision == LYNX_PREC_FP64 ? sizeof(double) : sizeof(float);
+    for (int i = 0; i < 3; ++i) LYNX_TRY(c->wbuf[i].ensure(esz * (size_t)Nd * ncol));
+    const bool nl = c->has_nl;
+    if (!with_nonlocal) c->has_nl = false;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st = LYNX_OK;
+    const float* v32 = nullptr;
+    if (precision == LYNX_PREC_MIXED) v32 = veff_as<float>(c, veff, &st);
+    for (int r = -1; r < reps && st == LYNX_OK; ++r) {  // r = -1: untimed warm-up launch
+        if (r == 0) cudaEventRecord(e0, c->stream);
+        const int a = (r + 3) % 3, b = (r + 4) % 3, o = (r + 5) % 3;
+        if (precision == LYNX_PREC_FP64)
+            st = cheb_step<double>(c, c->wbuf[a].as<double>(), Nd, c->wbuf[b].as<double>(), Nd,
+                                   c->wbuf[o].as<double>(), Nd, veff, ncol, 0.5, -0.1, -0.25, false);
+        else
+            st = cheb_step<float>(c, c->wbuf[a].as<float>(), Nd, c->wbuf[b].as<float>(), Nd,
+                                  c->wbuf[o].as<float>(), Nd, v32, ncol, 0.5, -0.1, -0.25, false);
+    }
+    cudaEventRecord(e1, c->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->has_nl = nl;
+    if (st != LYNX_OK) return st;
+    LYNX_CUDA_TRY(cudaGetLastError());
+    *ms_per_step = ms / reps;
+    return LYNX_OK;
+}
+
+int lynx_lanczos_bounds(lynx_ctx* c, const double* veff, double tol, int max_iter, double* emin, double* emax) {
+    return lanczos_impl<double>(c, veff, tol, max_iter, emin, emax, false);
+}
+
+int lynx_lanczos_bounds_kpt(lynx_ctx* c, const double* veff, double tol, int max_iter, double* emin, double* emax) {
+    return lanczos_impl<double2>(c, veff, tol, max_iter, emin, emax, true);
+}
+
+int lynx_fermi_level(const double* eigs, const double* w, int n, double ne, double beta, int smearing, double* ef) {
+    LYNX_CHECK_ARG(eigs && w && ef, "null pointer");
+    LYNX_CHECK_ARG(n > 0, "no eigenvalues for the Fermi level search");
+    LYNX_CHECK_ARG(beta > 0, "beta must be positive");
+    double emin = eigs[0], emax = eigs[0];
+    for (int i = 1; i < n; ++i) {
+        emin = std::min(emin, eigs[i]);
+        emax = std::max(emax, eigs[i]);
+    }
+    auto resid = [&](double x) {
+        double s = 0;
+        for (int i = 0; i < n; ++i) s += w[i] * smear(eigs[i] - x, beta, smearing);
+        return s - ne;
+    };
+    double a = emin - 10.0 / beta, b = emax + 10.0 / beta;
+    if (resid(a) * resid(b) > 0) {
+        a = emin - 100.0 / beta;
+        b = emax + 100.0 / beta;
+        if (resid(a) * resid(b) > 0) {
+            set_error("cannot bracket the Fermi level");
+            return LYNX_ERR_BRACKET;
+        }
+    }
+    *ef = brent_zero(resid, a, b, 1e-14, 200);
+    return LYNX_OK;
+}
+
+int lynx_occupations(const double* eigs, int n, double ef, double beta, int smearing, double* occ) {
+    LYNX_CHECK_ARG(eigs && occ, "null pointer");
+    for (int i = 0; i < n; ++i) occ[i] = smear(eigs[i] - ef, beta, smearing);
+    return LYNX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,317 @@
+"""Python mirror of the reference operator API on top of the lynx_b200 C ABI.
+
+Mirrors the pybind11 layer of the reference (python/src/bind_solvers.cpp:54-114,
+python/src/bind_operators.cpp:51-71) and python/lynx/ops/hamiltonian.py:
+same method names, argument meaning and return values.
+
+Orbitals can be passed two ways:
+  * host numpy arrays of shape (Nd, nband) (Fortran order, like the reference binding),
+    copied to the device for the call and back;
+  * device-resident torch tensors of shape (nband, Nd) (contiguous, i.e. column-major
+    Nd x nband), float64 or complex128, used in place on torch's current CUDA stream.
+torch is used for device memory and streams only; every operator runs in liblynxb200.so.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Tuple
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr, iptr
+from .cell import Cell
+from .pseudo import NonlocalTables
+
+_PREC = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+_SMEAR = {"fermi-dirac": _lib.SMEAR_FERMI_DIRAC, "fd": _lib.SMEAR_FERMI_DIRAC,
+          "gaussian": _lib.SMEAR_GAUSSIAN}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _is_torch(x) -> bool:
+    try:
+        import torch
+        return isinstance(x, torch.Tensor)
+    except ImportError:  # pragma: no cover
+        return False
+
+
+def _dev_ptr(t) -> int:
+    if not t.is_cuda:
+        raise ValueError("device tensors must live on a CUDA device")
+    if not t.is_contiguous():
+        raise ValueError("device tensors must be contiguous")
+    return t.data_ptr()
+
+
+class Context:
+    """One cell (grid, lattice, FD stencil, boundary conditions, projectors) on one GPU.
+
+    Replaces the reference's FDGrid/Lattice/FDStencil/HaloExchange set-up and
+    Hamiltonian::setup_gpu (see include/lynx_b200.h:lynx_create)."""
+
+    def __init__(self, cell: Cell, device: int = 0):
+        self.lib = _lib.load()
+        self.cell = cell
+        self.device = device
+        h = ctypes.c_void_p()
+        lat = np.ascontiguousarray(cell.latvec, dtype=np.float64)
+        bc = np.ascontiguousarray(cell.bc, dtype=np.int32)
+        nx, ny, nz = cell.shape
+        check(self.lib.lynx_create(ctypes.byref(h), device, nx, ny, nz, cell.fd_order, dptr(lat),
+                                   1 if cell.orthogonal else 0, iptr(bc)))
+        self._h = h
+        nd = ctypes.c_int()
+        dv = ctypes.c_double()
+        me = ctypes.c_double()
+        check(self.lib.lynx_grid_info(self._h, ctypes.byref(nd), ctypes.byref(dv), ctypes.byref(me)))
+        self.nd = nd.value
+        self.dV = dv.value
+        self.max_eigval_half_lap = me.value
+        self.has_nonlocal = False
+        self.kpt = np.zeros(3)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.lynx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync_stream(self):
+        """Point the context at torch's current CUDA stream."""
+        torch = _torch()
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        check(self.lib.lynx_set_stream(self._h, ctypes.c_void_p(s)))
+
+    def stencil_coeffs(self) -> dict:
+        n = self.cell.fd_order // 2 + 1
+        out = {k: np.zeros(n) for k in ("D2x", "D2y", "D2z", "D2xy", "D2xz", "D2yz", "D1x", "D1y", "D1z")}
+        check(self.lib.lynx_stencil_coeffs(self._h, *[dptr(out[k]) for k in
+                                                      ("D2x", "D2y", "D2z", "D2xy", "D2xz", "D2yz", "D1x", "D1y", "D1z")]))
+        return out
+
+    def set_nonlocal(self, tab: Optional[NonlocalTables]):
+        if tab is None or tab.n_img == 0:
+            check(self.lib.lynx_set_nonlocal(self._h, 0, None, None, None, None, None, 0, None, None))
+            self.has_nonlocal = False
+            return
+        a = np.ascontiguousarray(tab.img_atom, np.int32)
+        n = np.ascontiguousarray(tab.img_ndc, np.int32)
+        s = np.ascontiguousarray(tab.img_shift, np.float64)
+        g = np.ascontiguousarray(tab.gpos, np.int32)
+        c = np.ascontiguousarray(tab.chi, np.float64)
+        npj = np.ascontiguousarray(tab.atom_nproj, np.int32)
+        gm = np.ascontiguousarray(tab.gamma, np.float64)
+        check(self.lib.lynx_set_nonlocal(self._h, tab.n_img, iptr(a), iptr(n), dptr(s), iptr(g), dptr(c),
+                                         tab.n_atom, iptr(npj), dptr(gm)))
+        self.has_nonlocal = True
+
+    def set_kpoint(self, kcart):
+        k = np.ascontiguousarray(kcart, dtype=np.float64).reshape(3)
+        check(self.lib.lynx_set_kpoint(self._h, dptr(k)))
+        self.kpt = k.copy()
+
+
+class _DeviceArgs:
+    """Moves host numpy orbitals to the device for one call and back."""
+
+    def __init__(self, ctx: Context, psi, complex_: bool):
+        torch = _torch()
+        self.host = not _is_torch(psi)
+        self.complex = complex_
+        if self.host:
+            arr = np.asarray(psi)
+            self.one_d = arr.ndim == 1
+            arr2 = arr.reshape(arr.shape[0], -1, order="F")
+            if arr2.shape[0] != ctx.nd:
+                raise ValueError(f"psi has {arr2.shape[0]} rows, the grid has {ctx.nd} points")
+            dt = np.complex128 if complex_ else np.float64
+            cols = np.ascontiguousarray(arr2.T.astype(dt, copy=False))
+            self.t = torch.from_numpy(cols).to(f"cuda:{ctx.device}")
+        else:
+            self.one_d = psi.dim() == 1
+            self.t = psi.reshape(1, -1) if self.one_d else psi
+            if self.t.shape[-1] != ctx.nd:
+                raise ValueError(f"psi rows {self.t.shape[-1]} != grid points {ctx.nd}")
+        self.ncol = self.t.shape[0]
+
+    def like(self):
+        return _torch().empty_like(self.t)
+
+    def out(self, t):
+        if self.host:
+            a = t.cpu().numpy().T
+            a = np.asfortranarray(a)
+            return a[:, 0] if self.one_d else a
+        return t.reshape(-1) if self.one_d else t
+
+
+def _veff_dev(ctx: Context, Veff):
+    torch = _torch()
+    if _is_torch(Veff):
+        v = Veff.to(device=f"cuda:{ctx.device}", dtype=torch.float64).contiguous()
+    else:
+        v = torch.from_numpy(np.ascontiguousarray(Veff, dtype=np.float64)).to(f"cuda:{ctx.device}")
+    if v.numel() != ctx.nd:
+        raise ValueError("Veff must have Nd entries")
+    return v
+
+
+class NonlocalProjector:
+    """Vnl apply (NonlocalProjector::apply / apply_kpt): returns hpsi + Vnl psi."""
+
+    def __init__(self, ctx: Context, tables: Optional[NonlocalTables] = None):
+        self.ctx = ctx
+        if tables is not None:
+            ctx.set_nonlocal(tables)
+
+    def total_nproj(self) -> int:
+        return 0
+
+    def apply(self, psi, hpsi, kpt: bool = False):
+        ctx = self.ctx
+        ctx.sync_stream()
+        a = _DeviceArgs(ctx, psi, kpt)
+        h = _DeviceArgs(ctx, hpsi, kpt)
+        fn = ctx.lib.lynx_nonlocal_apply_kpt if kpt else ctx.lib.lynx_nonlocal_apply
+        check(fn(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), ctypes.c_void_p(_dev_ptr(h.t)), a.ncol, ctx.nd))
+        return h.out(h.t)
+
+
+class Hamiltonian:
+    """H psi = -0.5 Lap psi + Veff psi + Vnl psi (+ shift psi).
+
+    Mirrors lynx.ops.Hamiltonian (python/lynx/ops/hamiltonian.py:1-64) and the C++
+    Hamiltonian::apply / apply_kpt."""
+
+    def __init__(self, ctx: Context, Veff=None):
+        self.ctx = ctx
+        self._Veff = None if Veff is None else np.asarray(Veff, dtype=np.float64)
+
+    def set_potential(self, Veff):
+        self._Veff = Veff
+
+    def apply(self, psi, Veff=None, shift: float = 0.0):
+        return self._apply(psi, Veff, shift, False)
+
+    def apply_kpt(self, psi, Veff=None, shift: float = 0.0):
+        return self._apply(psi, Veff, shift, True)
+
+    def __call__(self, psi, Veff=None, shift: float = 0.0):
+        return self.apply(psi, Veff, shift)
+
+    def __matmul__(self, psi):
+        return self.apply(psi)
+
+    def _apply(self, psi, Veff, shift, kpt):
+        ctx = self.ctx
+        V = self._Veff if Veff is None else Veff
+        if V is None:
+            raise ValueError("No effective potential set. Call set_potential() first.")
+        ctx.sync_stream()
+        a = _DeviceArgs(ctx, psi, kpt)
+        v = _veff_dev(ctx, V)
+        y = a.like()
+        fn = ctx.lib.lynx_hamiltonian_apply_kpt if kpt else ctx.lib.lynx_hamiltonian_apply
+        check(fn(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), ctypes.c_void_p(v.data_ptr()),
+                 ctypes.c_void_p(_dev_ptr(y)), a.ncol, ctx.nd, float(shift)))
+        return a.out(y)
+
+
+class EigenSolver:
+    """Chebyshev-filtered subspace iteration (EigenSolver::solve / solve_kpt / lanczos_bounds).
+
+    solve(psi, Veff, lambda_cutoff, eigval_min, eigval_max, cheb_degree=20) -> (psi_out, eig),
+    the signature of the reference binding (python/src/bind_solvers.cpp:54-114).  Host numpy
+    psi is copied (the reference binding copies too); a device torch tensor is updated in place
+    and returned."""
+
+    def __init__(self, ctx: Context, precision: str = "fp64"):
+        self.ctx = ctx
+        self.precision = precision
+        self._lambda_cutoff = 0.0
+
+    def lambda_cutoff(self) -> float:
+        return self._lambda_cutoff
+
+    def set_lambda_cutoff(self, lc: float):
+        self._lambda_cutoff = float(lc)
+
+    def _solve(self, psi, Veff, lambda_cutoff, eigval_min, eigval_max, cheb_degree, precision, kpt):
+        ctx = self.ctx
+        prec = _PREC[precision or self.precision]
+        ctx.sync_stream()
+        a = _DeviceArgs(ctx, psi, kpt)
+        v = _veff_dev(ctx, Veff)
+        eig = np.zeros(a.ncol)
+        lc_out = ctypes.c_double()
+        fn = ctx.lib.lynx_eigensolver_solve_kpt if kpt else ctx.lib.lynx_eigensolver_solve
+        check(fn(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), dptr(eig), ctypes.c_void_p(v.data_ptr()), a.ncol,
+                 ctx.nd, float(lambda_cutoff), float(eigval_min), float(eigval_max), int(cheb_degree), prec,
+                 ctypes.byref(lc_out)))
+        self._lambda_cutoff = lc_out.value
+        return a.out(a.t), eig
+
+    def solve(self, psi, Veff, lambda_cutoff, eigval_min, eigval_max, cheb_degree: int = 20,
+              precision: Optional[str] = None):
+        return self._solve(psi, Veff, lambda_cutoff, eigval_min, eigval_max, cheb_degree, precision, False)
+
+    def solve_kpt(self, psi, Veff, lambda_cutoff, eigval_min, eigval_max, cheb_degree: int = 20,
+                  precision: Optional[str] = None):
+        return self._solve(psi, Veff, lambda_cutoff, eigval_min, eigval_max, cheb_degree, precision, True)
+
+    def chebyshev_filter(self, X, Veff, lambda_cutoff, eigval_min, eigval_max, degree: int = 20,
+                         precision: Optional[str] = None, kpt: bool = False):
+        ctx = self.ctx
+        ctx.sync_stream()
+        a = _DeviceArgs(ctx, X, kpt)
+        v = _veff_dev(ctx, Veff)
+        y = a.like()
+        fn = ctx.lib.lynx_chebyshev_filter_kpt if kpt else ctx.lib.lynx_chebyshev_filter
+        check(fn(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), ctypes.c_void_p(_dev_ptr(y)),
+                 ctypes.c_void_p(v.data_ptr()), a.ncol, ctx.nd, float(lambda_cutoff), float(eigval_min),
+                 float(eigval_max), int(degree), _PREC[precision or self.precision]))
+        return a.out(y)
+
+    def lanczos_bounds(self, Veff, tol: float = 1e-2, max_iter: int = 1000, kpt: bool = False) -> Tuple[float, float]:
+        ctx = self.ctx
+        ctx.sync_stream()
+        v = _veff_dev(ctx, Veff)
+        lo, hi = ctypes.c_double(), ctypes.c_double()
+        fn = ctx.lib.lynx_lanczos_bounds_kpt if kpt else ctx.lib.lynx_lanczos_bounds
+        check(fn(ctx.handle, ctypes.c_void_p(v.data_ptr()), float(tol), int(max_iter), ctypes.byref(lo),
+                 ctypes.byref(hi)))
+        return lo.value, hi.value
+
+
+def fermi_level(eigs, weights, nelectron: float, beta: float, smearing: str = "fermi-dirac") -> float:
+    """Occupation::find_fermi_level (src/electronic/Occupation.cpp:48-84)."""
+    lib = _lib.load()
+    e = np.ascontiguousarray(eigs, dtype=np.float64).ravel()
+    w = np.ascontiguousarray(weights, dtype=np.float64).ravel()
+    ef = ctypes.c_double()
+    check(lib.lynx_fermi_level(dptr(e), dptr(w), len(e), float(nelectron), float(beta), _SMEAR[smearing],
+                               ctypes.byref(ef)))
+    return ef.value
+
+
+def occupations(eigs, ef: float, beta: float, smearing: str = "fermi-dirac") -> np.ndarray:
+    lib = _lib.load()
+    e = np.ascontiguousarray(eigs, dtype=np.float64).ravel()
+    occ = np.zeros_like(e)
+    check(lib.lynx_occupations(dptr(e), len(e), float(ef), float(beta), _SMEAR[smearing], dptr(occ)))
+    return occ

@@ -1,0 +1,179 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference CPU hot path.
+
+The checker is oracle/_ref/libref_lynx.so: the reference LYNX EigenSolver /
+Hamiltonian / NonlocalProjector sources compiled unmodified.  Both sides get the
+same seeded inputs and the same projector tables.
+
+Tolerances (written per test):
+  * FP64 operators (H psi, Vnl psi, filter): max |diff| / max |ref| <= 1e-12 (stencil)
+    and <= 1e-10 (degree-m filter, where the recurrence amplifies rounding);
+  * FP64 CheFSI pass: Ritz values within 1e-9 Ha, Ritz subspaces within 1e-7;
+  * FP32 filter (mixed precision): relative 2e-5 per filter block.
+"""
+import numpy as np
+import pytest
+
+from helpers import rel_err, si8_small, subspace_distance
+from lynx_b200 import cell as C
+from lynx_b200 import pseudo as P
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def system(synth_psp8):
+    import torch
+    from lynx_b200 import solver
+    cl, pos, V = si8_small()
+    R = ref.RefLynx(cl, pos, synth_psp8)
+    ctx = solver.Context(cl)
+    tab = P.nonlocal_tables(cl, pos, P.read_psp8(synth_psp8))
+    ctx.set_nonlocal(tab)
+    return dict(cell=cl, pos=pos, V=V, R=R, ctx=ctx, solver=solver, torch=torch)
+
+
+def test_grid_matches_reference(system):
+    R, ctx = system["R"], system["ctx"]
+    assert ctx.nd == R.nd
+    assert abs(ctx.dV - R.dV) < 1e-15
+    st = R.stencil()
+    mine = ctx.stencil_coeffs()
+    for k in ("D2x", "D2y", "D2z", "D1x", "D1y", "D1z"):
+        np.testing.assert_allclose(mine[k], st[k], rtol=1e-14, atol=1e-14)
+    assert abs(ctx.max_eigval_half_lap - st["max_eigval"]) < 1e-12
+
+
+@pytest.mark.parametrize("ncol,shift", [(1, 0.0), (5, 0.0), (3, 0.37)])
+def test_hamiltonian_apply_real(system, ncol, shift):
+    s = system
+    psi = C.random_orbitals(s["ctx"].nd, ncol, seed=11 + ncol)
+    y_ref = s["R"].h_apply(psi, s["V"], shift)
+    y = s["solver"].Hamiltonian(s["ctx"], s["V"]).apply(psi, shift=shift)
+    assert rel_err(y, y_ref) < 1e-12
+
+
+def test_hamiltonian_apply_device_tensor(system):
+    s = system
+    torch = s["torch"]
+    psi = C.random_orbitals(s["ctx"].nd, 4, seed=5)
+    y_ref = s["R"].h_apply(psi, s["V"])
+    t = torch.from_numpy(np.ascontiguousarray(psi.T)).cuda()
+    y = s["solver"].Hamiltonian(s["ctx"]).apply(t, Veff=torch.from_numpy(s["V"]).cuda())
+    assert y.shape == t.shape and y.is_cuda
+    assert rel_err(y.cpu().numpy().T, y_ref) < 1e-12
+
+
+def test_hamiltonian_apply_kpt(system):
+    s = system
+    cl = s["cell"]
+    k = np.array([0.11, -0.23, 0.31]) * 2 * np.pi / cl.lengths
+    psi = C.random_orbitals(s["ctx"].nd, 3, seed=7, complex_=True)
+    y_ref = s["R"].h_apply_kpt(psi, s["V"], k, 0.1)
+    s["ctx"].set_kpoint(k)
+    y = s["solver"].Hamiltonian(s["ctx"], s["V"]).apply_kpt(psi, shift=0.1)
+    assert rel_err(y, y_ref) < 1e-12
+
+
+def test_nonlocal_apply(system):
+    s = system
+    psi = C.random_orbitals(s["ctx"].nd, 6, seed=9)
+    h0 = C.random_orbitals(s["ctx"].nd, 6, seed=10)
+    y_ref = s["R"].nl_apply(psi, h0)
+    y = s["solver"].NonlocalProjector(s["ctx"]).apply(psi, np.array(h0))
+    assert rel_err(y, y_ref) < 1e-12
+
+
+def _bounds(s):
+    lo, hi = s["R"].lanczos(s["V"])
+    return lo, hi, 0.5 * (lo + hi)
+
+
+def test_lanczos_bounds(system):
+    s = system
+    lo_r, hi_r = s["R"].lanczos(s["V"])
+    lo, hi = s["solver"].EigenSolver(s["ctx"]).lanczos_bounds(s["V"])
+    assert abs(lo - lo_r) < 1e-6 * max(1.0, abs(lo_r))
+    assert abs(hi - hi_r) < 1e-6 * abs(hi_r)
+
+
+@pytest.mark.parametrize("degree", [1, 2, 7])
+def test_chebyshev_filter_fp64(system, degree):
+    s = system
+    lo, hi, lc = _bounds(s)
+    X = C.random_orbitals(s["ctx"].nd, 6, seed=21)
+    Y_ref = s["R"].chebyshev_filter(X, s["V"], lc, lo, hi, degree)
+    Y = s["solver"].EigenSolver(s["ctx"]).chebyshev_filter(X, s["V"], lc, lo, hi, degree, precision="fp64")
+    assert rel_err(Y, Y_ref) < 1e-10
+
+
+def test_chebyshev_filter_mixed(system):
+    s = system
+    lo, hi, lc = _bounds(s)
+    X = C.random_orbitals(s["ctx"].nd, 6, seed=21)
+    Y_ref = s["R"].chebyshev_filter(X, s["V"], lc, lo, hi, 12)
+    Y = s["solver"].EigenSolver(s["ctx"]).chebyshev_filter(X, s["V"], lc, lo, hi, 12, precision="mixed")
+    for j in range(6):  # per column, relative to the column's own scale
+        assert rel_err(Y[:, j], Y_ref[:, j]) < 2e-5
+
+
+def test_chebyshev_filter_kpt(system):
+    s = system
+    cl = s["cell"]
+    k = np.array([0.25, 0.0, -0.25]) * 2 * np.pi / cl.lengths
+    lo, hi = s["R"].lanczos(s["V"], kpt=k)
+    lc = 0.5 * (lo + hi)
+    X = C.random_orbitals(s["ctx"].nd, 4, seed=33, complex_=True)
+    Y_ref = s["R"].chebyshev_filter_kpt(X, s["V"], lc, lo, hi, 8, k)
+    s["ctx"].set_kpoint(k)
+    Y = s["solver"].EigenSolver(s["ctx"]).chebyshev_filter(X, s["V"], lc, lo, hi, 8, precision="fp64", kpt=True)
+    assert rel_err(Y, Y_ref) < 1e-10
+
+
+def test_solve_fp64_matches_reference(system):
+    s = system
+    lo, hi, lc = _bounds(s)
+    N = 16
+    psi0 = C.random_orbitals(s["ctx"].nd, N, seed=41)
+    psi_r, eig_r = s["R"].solve(psi0, s["V"], lc, lo, hi, 20)
+    es = s["solver"].EigenSolver(s["ctx"], "fp64")
+    psi, eig = es.solve(psi0, s["V"], lc, lo, hi, 20)
+    assert np.all(np.diff(eig) >= -1e-12)
+    assert np.abs(eig - eig_r).max() < 1e-9
+    assert abs(es.lambda_cutoff() - (eig[-1] + 0.1)) < 1e-12
+    assert subspace_distance(psi, psi_r) < 1e-7
+
+
+def test_solve_kpt_fp64_matches_reference(system):
+    s = system
+    cl = s["cell"]
+    k = np.array([0.25, 0.25, 0.0]) * 2 * np.pi / cl.lengths
+    lo, hi = s["R"].lanczos(s["V"], kpt=k)
+    lc = 0.5 * (lo + hi)
+    N = 10
+    psi0 = C.random_orbitals(s["ctx"].nd, N, seed=43, complex_=True)
+    psi_r, eig_r = s["R"].solve_kpt(psi0, s["V"], lc, lo, hi, 16, k)
+    s["ctx"].set_kpoint(k)
+    psi, eig = s["solver"].EigenSolver(s["ctx"], "fp64").solve_kpt(psi0, s["V"], lc, lo, hi, 16)
+    assert np.abs(eig - eig_r).max() < 1e-9
+    assert subspace_distance(psi, psi_r) < 1e-7
+
+
+def test_scf_like_convergence_mixed_vs_fp64(system):
+    """Repeated CheFSI passes at fixed V (the SCF inner loop): the mixed-precision
+    path converges to the same occupied Ritz values as the FP64 path (<= 1e-6 Ha)."""
+    s = system
+    lo, hi, lc0 = _bounds(s)
+    N = 16
+    out = {}
+    for prec in ("fp64", "mixed"):
+        es = s["solver"].EigenSolver(s["ctx"], prec)
+        psi = C.random_orbitals(s["ctx"].nd, N, seed=77)
+        lc, emin = lc0, lo
+        for it in range(12):
+            psi, eig = es.solve(psi, s["V"], lc, emin, hi, 20)
+            lc = es.lambda_cutoff()
+            emin = eig[0]
+        out[prec] = eig
+    nocc = 12
+    assert np.abs(out["mixed"][:nocc] - out["fp64"][:nocc]).max() < 1e-6
