@@ -166,8 +166,24 @@ struct lynx_ctx {
 
 namespace {
 
+// Makes the context's device current and creates the cuBLAS / cuSOLVER handles on first
+// use, so that lynx_create itself needs no GPU (set-up queries work on a CPU-only host).
 int activate(lynx_ctx* c) {
     LYNX_CUDA_TRY(cudaSetDevice(c->device));
+    if (!c->cublas) {
+        if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS) {
+            c->cublas = nullptr;
+            set_error("cuBLAS initialisation failed");
+            return LYNX_ERR_CUDA;
+        }
+    }
+    if (!c->cusolver) {
+        if (cusolverDnCreate(&c->cusolver) != CUSOLVER_STATUS_SUCCESS) {
+            c->cusolver = nullptr;
+            set_error("cuSOLVER initialisation failed");
+            return LYNX_ERR_CUDA;
+        }
+    }
     return LYNX_OK;
 }
 
@@ -659,10 +675,19 @@ int lanczos_impl(lynx_ctx* c, const double* veff, double tol, int max_iter, doub
     double* vjm1 = c->lz[0].as<double>();
     double* vj = c->lz[1].as<double>();
     double* vp1 = c->lz[2].as<double>();
-    // Start vector: srand(1); entries rand()/RAND_MAX (re, im interleaved for complex).
+    // Start vector: srand(1); entries rand()/RAND_MAX.  For complex entries the reference
+    // writes Complex(rand()/RAND_MAX, rand()/RAND_MAX), whose GCC build draws the imaginary
+    // part first; the same order is kept so both start from the same vector.
     std::vector<double> h(Nv);
     std::srand(1);
-    for (long long i = 0; i < Nv; ++i) h[i] = (double)std::rand() / RAND_MAX;
+    if (cplx) {
+        for (long long i = 0; i < Nv; i += 2) {
+            h[i + 1] = (double)std::rand() / RAND_MAX;
+            h[i] = (double)std::rand() / RAND_MAX;
+        }
+    } else {
+        for (long long i = 0; i < Nv; ++i) h[i] = (double)std::rand() / RAND_MAX;
+    }
     double nrm = 0;
     for (double v : h) nrm += v * v;
     const double sc = 1.0 / std::sqrt(nrm);
@@ -845,27 +870,18 @@ int lynx_create(lynx_ctx** out, int device, int nx, int ny, int nz, int fd_order
         set_error("lattice vectors are coplanar");
         return LYNX_ERR_BAD_ARG;
     }
-    cudaError_t e = cudaSetDevice(device);
-    if (e != cudaSuccess) {
-        delete c;
-        set_error("cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
-        return LYNX_ERR_CUDA;
-    }
-    if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS || cusolverDnCreate(&c->cusolver) != CUSOLVER_STATUS_SUCCESS) {
-        if (c->cublas) cublasDestroy(c->cublas);
-        delete c;
-        set_error("cuBLAS/cuSOLVER initialisation failed");
-        return LYNX_ERR_CUDA;
-    }
     *out = c;
     return LYNX_OK;
 }
 
 int lynx_destroy(lynx_ctx* c) {
     if (!c) return LYNX_OK;
-    cudaSetDevice(c->device);
-    if (c->stream) cudaStreamSynchronize(c->stream);
-    else cudaDeviceSynchronize();
+    const bool used = c->cublas != nullptr;  // the device was touched by this context
+    if (used) {
+        cudaSetDevice(c->device);
+        if (c->stream) cudaStreamSynchronize(c->stream);
+        else cudaDeviceSynchronize();
+    }
     for (auto& b : c->wbuf) b.release();
     for (auto& b : c->cvt) b.release();
     for (auto& b : c->lz) b.release();
