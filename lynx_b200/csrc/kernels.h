@@ -21,6 +21,19 @@ int launch_cheb_step(const StencilGeom& g, const T* x, long long ldx, const T* x
                      long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl,
                      const T* phr, cudaStream_t st);
 
+// Padded row length used by the pipelined stencil: rows and Veff rows must be 16-byte multiples.
+inline int pipe_row_elems(int nx, size_t scalar_size) {
+    const int q = (int)(16 / scalar_size);
+    return ((nx + q - 1) / q) * q;
+}
+
+// Pipelined stencil on 16-byte aligned, row-padded (nxp) blocks; V padded the same way.
+// err: device int set to 1 if a bounded shared-memory wait gives up.
+template <typename T, typename S>
+int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out,
+                     long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl, const T* phr,
+                     int* err, cudaStream_t st);
+
 // Launches issued by the library (diagnostic counter, incremented by every launcher).
 void count_launch(int n = 1);
 

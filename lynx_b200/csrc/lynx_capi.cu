@@ -21,6 +21,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -162,6 +163,12 @@ struct lynx_ctx {
     DevBuf Ms, Hs, eigd, solver_work, info;
     DevBuf lz[4];         // Lanczos vectors
     DevBuf io_psi, io_v;  // staging for the host-pointer solve
+    DevBuf vpad64, vpad32;  // Veff in the padded row layouts of the pipelined stencil
+    DevBuf errflag;         // set by a kernel whose bounded wait gave up
+    // nonlocal tables re-indexed for padded row layouts: nxp -> tables
+    std::map<int, NLDev> nl_layouts;
+    std::vector<DevBuf> nl_layout_bufs;
+    std::vector<int> h_gpos, h_pt_grid;  // host copies of the unpadded grid indices
 };
 
 namespace {
@@ -354,51 +361,158 @@ template <> struct Real<float> { using type = float; };
 template <> struct Real<double2> { using type = double; };
 template <> struct Real<float2> { using type = float; };
 
-// V (FP64 device) in the scalar type of T.
-template <typename S> const S* veff_as(lynx_ctx* c, const double* v, int* st);
-template <> const double* veff_as<double>(lynx_ctx*, const double* v, int* st) {
-    *st = LYNX_OK;
-    return v;
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// Grows a work buffer; new storage is zeroed so that the padding elements of padded
+// row layouts read as zero.
+int ensure_zeroed(lynx_ctx* c, DevBuf& b, size_t bytes) {
+    if (bytes <= b.bytes) return LYNX_OK;
+    LYNX_TRY(b.ensure(bytes));
+    LYNX_CUDA_TRY(cudaMemsetAsync(b.p, 0, b.bytes, c->stream));
+    return LYNX_OK;
 }
-template <> const float* veff_as<float>(lynx_ctx* c, const double* v, int* st) {
-    *st = c->v32.ensure(sizeof(float) * c->Nd);
-    if (*st) return nullptr;
-    *st = convert_cols<float, double>(c->v32.as<float>(), c->Nd, v, c->Nd, c->Nd, 1, c->stream);
-    return c->v32.as<float>();
+
+// Copy/convert the valid points of ncol columns between row layouts (row length nxp, column stride ld).
+template <typename Dst, typename Src>
+__global__ void repack_kernel(Dst* __restrict__ dst, int dnxp, long long dld, const Src* __restrict__ src, int snxp,
+                              long long sld, int nx, long long nrows, int ncol) {
+    const long long per_col = (long long)nx * nrows;
+    const long long total = per_col * ncol;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long cidx = i / per_col;
+        const long long rem = i - cidx * per_col;
+        const long long r = rem / nx;
+        const int xi = (int)(rem - r * nx);
+        cvt_val(dst[cidx * dld + r * dnxp + xi], src[cidx * sld + r * snxp + xi]);
+    }
+}
+
+template <typename Dst, typename Src>
+int repack(lynx_ctx* c, Dst* dst, int dnxp, long long dld, const Src* src, int snxp, long long sld, int ncol) {
+    const long long total = (long long)c->nx * c->ny * c->nz * ncol;
+    if (total == 0) return LYNX_OK;
+    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
+    repack_kernel<Dst, Src><<<blocks, 256, 0, c->stream>>>(dst, dnxp, dld, src, snxp, sld, c->nx,
+                                                           (long long)c->ny * c->nz, ncol);
+    count_launch();
+    LYNX_CUDA_TRY(cudaGetLastError());
+    return LYNX_OK;
+}
+
+// Nonlocal tables whose grid indices address rows of length nxp.
+int nl_for(lynx_ctx* c, int nxp, const NLDev** out) {
+    if (nxp == c->nx) {
+        *out = &c->nl;
+        return LYNX_OK;
+    }
+    auto it = c->nl_layouts.find(nxp);
+    if (it != c->nl_layouts.end()) {
+        *out = &it->second;
+        return LYNX_OK;
+    }
+    auto remap = [&](const std::vector<int>& g) {
+        std::vector<int> r(g.size());
+        for (size_t i = 0; i < g.size(); ++i) {
+            const int xi = g[i] % c->nx;
+            const int rest = g[i] / c->nx;
+            r[i] = xi + nxp * rest;
+        }
+        return r;
+    };
+    NLDev d = c->nl;
+    const std::vector<int> gp = remap(c->h_gpos), pg = remap(c->h_pt_grid);
+    c->nl_layout_bufs.emplace_back();
+    DevBuf& b1 = c->nl_layout_bufs.back();
+    LYNX_TRY(b1.ensure(std::max<size_t>(gp.size() * 4, 16)));
+    LYNX_CUDA_TRY(cudaMemcpy(b1.p, gp.data(), gp.size() * 4, cudaMemcpyHostToDevice));
+    d.gpos = b1.as<int>();
+    c->nl_layout_bufs.emplace_back();
+    DevBuf& b2 = c->nl_layout_bufs.back();
+    LYNX_TRY(b2.ensure(std::max<size_t>(pg.size() * 4, 16)));
+    LYNX_CUDA_TRY(cudaMemcpy(b2.p, pg.data(), pg.size() * 4, cudaMemcpyHostToDevice));
+    d.pt_grid = b2.as<int>();
+    c->nl_layouts[nxp] = d;
+    *out = &c->nl_layouts[nxp];
+    return LYNX_OK;
+}
+
+// Veff (FP64, Nd, device) in scalar type S with rows of length nxp.
+template <typename S>
+int veff_layout(lynx_ctx* c, const double* v, int nxp, const S** out) {
+    if (std::is_same<S, double>::value && nxp == c->nx && aligned16(v)) {
+        *out = reinterpret_cast<const S*>(v);
+        return LYNX_OK;
+    }
+    DevBuf& b = std::is_same<S, double>::value ? c->vpad64 : c->vpad32;
+    LYNX_TRY(ensure_zeroed(c, b, sizeof(S) * (size_t)nxp * c->ny * c->nz));
+    LYNX_TRY(repack<S, double>(c, b.as<S>(), nxp, 0, v, c->nx, 0, 1));
+    *out = b.as<S>();
+    return LYNX_OK;
+}
+
+int check_errflag(lynx_ctx* c) {
+    if (!c->errflag.p) return LYNX_OK;
+    int h = 0;
+    LYNX_CUDA_TRY(cudaMemcpyAsync(&h, c->errflag.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (h) {
+        cudaMemsetAsync(c->errflag.p, 0, sizeof(int), c->stream);
+        set_error("a bounded device-side wait gave up (shared-memory pipeline did not complete)");
+        return LYNX_ERR_TIMEOUT;
+    }
+    return LYNX_OK;
 }
 
 // One fused step: out = a*(H_loc x) + b*x + d*xold, plus the nonlocal part a*Vnl x.
+// Blocks use rows of length nxp (nxp == nx: the caller's unpadded layout); V uses the same rows.
+// 16-byte aligned layouts run the pipelined kernel, others the register-window kernel.
 template <typename T>
-int cheb_step(lynx_ctx* c, const T* x, long long ldx, const T* xold, long long ldo, T* out, long long ldout,
+int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out, long long ldout,
               const typename Real<T>::type* V, int ncol, double a, double b, double d, bool use_k) {
     using S = typename Real<T>::type;
     T phl[3], phr[3];
     ghost_phases<T>(c, use_k, phl, phr);
-    const int ncolp = ((ncol + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
-    if (c->has_nl) {
-        LYNX_TRY(c->alpha.ensure(sizeof(T) * (size_t)c->nl.total_proj * ncolp));
-        LYNX_TRY(launch_nl_gather<T>(c->nl, x, ldx, ncol, c->alpha.as<T>(), ncolp, c->dV, c->stream));
+    const bool pipe_ok = (nxp * sizeof(S)) % 16 == 0 && (ldx * sizeof(T)) % 16 == 0 &&
+                         (ldout * sizeof(T)) % 16 == 0 && (!xold || (ldo * sizeof(T)) % 16 == 0) && aligned16(x) &&
+                         aligned16(out) && (!xold || aligned16(xold)) && aligned16(V);
+    if (!pipe_ok && nxp != c->nx) {
+        set_error("internal error: padded layout that is not 16-byte aligned");
+        return LYNX_ERR_BAD_ARG;
     }
-    LYNX_TRY(launch_cheb_step<T, S>(geom(c), x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, c->stream));
+    const int ncolp = ((ncol + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
+    const NLDev* nl = nullptr;
+    if (c->has_nl) {
+        LYNX_TRY(nl_for(c, nxp, &nl));
+        LYNX_TRY(c->alpha.ensure(sizeof(T) * (size_t)c->nl.total_proj * ncolp));
+        LYNX_TRY(launch_nl_gather<T>(*nl, x, ldx, ncol, c->alpha.as<T>(), ncolp, c->dV, c->stream));
+    }
+    if (pipe_ok) {
+        if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
+        LYNX_TRY(launch_cheb_pipe<T, S>(geom(c), nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
+                                        c->errflag.as<int>(), c->stream));
+    } else {
+        LYNX_TRY(launch_cheb_step<T, S>(geom(c), x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, c->stream));
+    }
     if (c->has_nl)
-        LYNX_TRY(launch_nl_scatter<T, S>(c->nl, out, ldout, ncol, c->alpha.as<T>(), ncolp, (S)a, c->stream));
+        LYNX_TRY(launch_nl_scatter<T, S>(*nl, out, ldout, ncol, c->alpha.as<T>(), ncolp, (S)a, c->stream));
     return LYNX_OK;
 }
 
-// Chebyshev filter (src/solvers/EigenSolver.cpp:559-619) on blocks of type T.
-// X is read at the first two steps only; bufs[0..2] rotate.  Returns the block
-// holding the filtered Y in *yout.
+// Chebyshev filter (src/solvers/EigenSolver.cpp:559-619) on blocks of type T with rows of
+// length nxp.  X (column stride ldX) is read at the first two steps only; bufs[0..2]
+// (column stride ldb) rotate.  Returns the block holding the filtered Y in *yout.
 template <typename T>
-int filter_blocks(lynx_ctx* c, const T* X, long long ldX, T* bufs[3], const typename Real<T>::type* V, int ncol,
-                  double lc, double emin, double emax, int degree, bool use_k, T** yout) {
-    const long long ld = c->Nd;
+int filter_blocks(lynx_ctx* c, int nxp, const T* X, long long ldX, T* bufs[3], long long ldb,
+                  const typename Real<T>::type* V, int ncol, double lc, double emin, double emax, int degree,
+                  bool use_k, T** yout) {
     const double e = (emax - lc) / 2.0;
     const double cc = (emax + lc) / 2.0;
     const double sigma1 = e / (emin - cc);
     double sigma = sigma1;
     // Y = (sigma1/e) (H X - c X)
     const double s0 = sigma1 / e;
-    LYNX_TRY(cheb_step<T>(c, X, ldX, nullptr, 0, bufs[0], ld, V, ncol, s0, -cc * s0, 0.0, use_k));
+    LYNX_TRY(cheb_step<T>(c, nxp, X, ldX, nullptr, 0, bufs[0], ldb, V, ncol, s0, -cc * s0, 0.0, use_k));
     const T* xold = X;
     long long ldold = ldX;
     int iy = 0;
@@ -406,10 +520,10 @@ int filter_blocks(lynx_ctx* c, const T* X, long long ldX, T* bufs[3], const type
         const double sigma_new = 1.0 / (2.0 / sigma1 - sigma);
         const double gamma = 2.0 * sigma_new / e;
         const int inew = (iy + 1) % 3;
-        LYNX_TRY(cheb_step<T>(c, bufs[iy], ld, xold, ldold, bufs[inew], ld, V, ncol, gamma, -gamma * cc,
+        LYNX_TRY(cheb_step<T>(c, nxp, bufs[iy], ldb, xold, ldold, bufs[inew], ldb, V, ncol, gamma, -gamma * cc,
                               -sigma * sigma_new, use_k));
         xold = bufs[iy];
-        ldold = ld;
+        ldold = ldb;
         iy = inew;
         sigma = sigma_new;
     }
@@ -417,6 +531,62 @@ int filter_blocks(lynx_ctx* c, const T* X, long long ldX, T* bufs[3], const type
     return LYNX_OK;
 }
 
+
+// Filter of the caller's FP64 block X (unpadded rows, column stride ldX) in FP64, on internal
+// blocks with rows of length nxp (16-byte multiples).  *Y (and *HY = H*Y when requested) are
+// left in internal storage with column stride *ldb.
+template <typename T64>
+int run_filter64(lynx_ctx* c, const T64* X, long long ldX, const double* veff, int N, double lc, double emin,
+                 double emax, int degree, bool use_k, bool want_hy, T64** Y, T64** HY, long long* ldb, int* nxp) {
+    using S = typename Real<T64>::type;
+    *nxp = pipe_row_elems(c->nx, sizeof(S));
+    *ldb = (long long)(*nxp) * c->ny * c->nz;
+    const size_t blk = sizeof(T64) * (size_t)(*ldb) * N;
+    const bool direct = (*nxp == c->nx) && (ldX * sizeof(T64)) % 16 == 0 && aligned16(X);
+    for (int i = 0; i < (direct ? 3 : 4); ++i) LYNX_TRY(ensure_zeroed(c, c->wbuf[i], blk));
+    const S* Vp = nullptr;
+    LYNX_TRY(veff_layout<S>(c, veff, *nxp, &Vp));
+    const T64* Xin = X;
+    long long ldin = ldX;
+    if (!direct) {
+        LYNX_TRY(repack<T64, T64>(c, c->wbuf[3].as<T64>(), *nxp, *ldb, X, c->nx, ldX, N));
+        Xin = c->wbuf[3].as<T64>();
+        ldin = *ldb;
+    }
+    T64* bufs[3] = {c->wbuf[0].as<T64>(), c->wbuf[1].as<T64>(), c->wbuf[2].as<T64>()};
+    LYNX_TRY(filter_blocks<T64>(c, *nxp, Xin, ldin, bufs, *ldb, Vp, N, lc, emin, emax, degree, use_k, Y));
+    if (want_hy) {
+        *HY = (*Y == bufs[0]) ? bufs[1] : bufs[0];
+        LYNX_TRY(cheb_step<T64>(c, *nxp, *Y, *ldb, nullptr, 0, *HY, *ldb, Vp, N, 1.0, 0.0, 0.0, use_k));
+    }
+    return LYNX_OK;
+}
+
+// Same in FP32 (T32 = float / float2) from the caller's FP64 block.
+template <typename T32, typename T64>
+int run_filter32(lynx_ctx* c, const T64* X, long long ldX, const double* veff, int N, double lc, double emin,
+                 double emax, int degree, bool use_k, bool want_hy, T32** Y, T32** HY, long long* ldb, int* nxp) {
+    using S = typename Real<T32>::type;
+    *nxp = pipe_row_elems(c->nx, sizeof(S));
+    *ldb = (long long)(*nxp) * c->ny * c->nz;
+    const size_t blk = sizeof(T32) * (size_t)(*ldb) * N;
+    for (int i = 0; i < 4; ++i) LYNX_TRY(ensure_zeroed(c, c->wbuf[i], blk));
+    const S* Vp = nullptr;
+    LYNX_TRY(veff_layout<S>(c, veff, *nxp, &Vp));
+    T32* X32 = c->wbuf[3].as<T32>();
+    LYNX_TRY(repack<T32, T64>(c, X32, *nxp, *ldb, X, c->nx, ldX, N));
+    T32* bufs[3] = {c->wbuf[0].as<T32>(), c->wbuf[1].as<T32>(), c->wbuf[2].as<T32>()};
+    LYNX_TRY(filter_blocks<T32>(c, *nxp, X32, *ldb, bufs, *ldb, Vp, N, lc, emin, emax, degree, use_k, Y));
+    if (want_hy) {
+        *HY = (*Y == bufs[0]) ? bufs[1] : bufs[0];
+        LYNX_TRY(cheb_step<T32>(c, *nxp, *Y, *ldb, nullptr, 0, *HY, *ldb, Vp, N, 1.0, 0.0, 0.0, use_k));
+    }
+    return LYNX_OK;
+}
+
+}  // namespace
+
+namespace {
 // ---------------------------------------------------------------------------
 // Rayleigh-Ritz in FP64 (cuBLAS / cuSOLVER), real and complex.
 // ---------------------------------------------------------------------------
@@ -575,36 +745,33 @@ int solve_impl(lynx_ctx* c, T64* psi, double* eig, const double* veff, int N, in
     const long long Nd = c->Nd;
     const long long ldp = ld > 0 ? ld : Nd;
     LYNX_CHECK_ARG(ldp >= Nd, "ld < Nd");
+    const size_t blk64 = sizeof(T64) * (size_t)Nd * N;
+    long long ldb = 0;
+    int nxp = 0;
     if (precision == LYNX_PREC_FP64) {
-        const size_t blk = sizeof(T64) * (size_t)Nd * N;
-        for (int i = 0; i < 3; ++i) LYNX_TRY(c->wbuf[i].ensure(blk));
-        T64* bufs[3] = {c->wbuf[0].as<T64>(), c->wbuf[1].as<T64>(), c->wbuf[2].as<T64>()};
-        T64* Y = nullptr;
-        LYNX_TRY(filter_blocks<T64>(c, psi, ldp, bufs, veff, N, lc, emin, emax, degree, use_k, &Y));
-        T64* HY = (Y == bufs[0]) ? bufs[1] : bufs[0];
-        LYNX_TRY(cheb_step<T64>(c, Y, Nd, nullptr, 0, HY, Nd, veff, N, 1.0, 0.0, 0.0, use_k));
-        LYNX_TRY(rayleigh_ritz(c, Y, Nd, HY, Nd, psi, ldp, N, eig));
+        T64 *Y = nullptr, *HY = nullptr;
+        LYNX_TRY(run_filter64<T64>(c, psi, ldp, veff, N, lc, emin, emax, degree, use_k, true, &Y, &HY, &ldb, &nxp));
+        if (nxp == c->nx) {
+            LYNX_TRY(rayleigh_ritz(c, Y, ldb, HY, ldb, psi, ldp, N, eig));
+        } else {
+            LYNX_TRY(c->cvt[0].ensure(blk64));
+            LYNX_TRY(c->cvt[1].ensure(blk64));
+            LYNX_TRY(repack<T64, T64>(c, c->cvt[0].as<T64>(), c->nx, Nd, Y, nxp, ldb, N));
+            LYNX_TRY(repack<T64, T64>(c, c->cvt[1].as<T64>(), c->nx, Nd, HY, nxp, ldb, N));
+            LYNX_TRY(rayleigh_ritz(c, c->cvt[0].as<T64>(), Nd, c->cvt[1].as<T64>(), Nd, psi, ldp, N, eig));
+        }
     } else {
-        int st = LYNX_OK;
-        const float* v32 = veff_as<float>(c, veff, &st);
-        if (st) return st;
-        const size_t blk = sizeof(T32) * (size_t)Nd * N;
-        for (int i = 0; i < 4; ++i) LYNX_TRY(c->wbuf[i].ensure(blk));
-        T32* X32 = c->wbuf[3].as<T32>();
-        LYNX_TRY(convert_cols<T32, T64>(X32, Nd, psi, ldp, Nd, N, c->stream));
-        T32* bufs[3] = {c->wbuf[0].as<T32>(), c->wbuf[1].as<T32>(), c->wbuf[2].as<T32>()};
-        T32* Y = nullptr;
-        LYNX_TRY(filter_blocks<T32>(c, X32, Nd, bufs, v32, N, lc, emin, emax, degree, use_k, &Y));
-        T32* HY = (Y == bufs[0]) ? bufs[1] : bufs[0];
-        LYNX_TRY(cheb_step<T32>(c, Y, Nd, nullptr, 0, HY, Nd, v32, N, 1.0, 0.0, 0.0, use_k));
+        T32 *Y = nullptr, *HY = nullptr;
+        LYNX_TRY(run_filter32<T32, T64>(c, psi, ldp, veff, N, lc, emin, emax, degree, use_k, true, &Y, &HY, &ldb,
+                                        &nxp));
         // Rayleigh-Ritz products on FP64 copies of the FP32 blocks.
-        const size_t blk64 = sizeof(T64) * (size_t)Nd * N;
         LYNX_TRY(c->cvt[0].ensure(blk64));
         LYNX_TRY(c->cvt[1].ensure(blk64));
-        LYNX_TRY(convert_cols<T64, T32>(c->cvt[0].as<T64>(), Nd, Y, Nd, Nd, N, c->stream));
-        LYNX_TRY(convert_cols<T64, T32>(c->cvt[1].as<T64>(), Nd, HY, Nd, Nd, N, c->stream));
+        LYNX_TRY(repack<T64, T32>(c, c->cvt[0].as<T64>(), c->nx, Nd, Y, nxp, ldb, N));
+        LYNX_TRY(repack<T64, T32>(c, c->cvt[1].as<T64>(), c->nx, Nd, HY, nxp, ldb, N));
         LYNX_TRY(rayleigh_ritz(c, c->cvt[0].as<T64>(), Nd, c->cvt[1].as<T64>(), Nd, psi, ldp, N, eig));
     }
+    LYNX_TRY(check_errflag(c));
     if (lc_out) *lc_out = eig[N - 1] + 0.1;
     return LYNX_OK;
 }
@@ -694,9 +861,11 @@ int lanczos_impl(lynx_ctx* c, const double* veff, double tol, int max_iter, doub
     for (double& v : h) v *= sc;
     LYNX_CUDA_TRY(cudaMemcpyAsync(vjm1, h.data(), Nv * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CUBLAS_TRY(cublasSetStream(c->cublas, c->stream));
+    const double* Vl = nullptr;
+    LYNX_TRY(veff_layout<double>(c, veff, c->nx, &Vl));
     auto Happly = [&](const double* x, double* y) -> int {
-        return cheb_step<T>(c, reinterpret_cast<const T*>(x), c->Nd, nullptr, 0, reinterpret_cast<T*>(y), c->Nd,
-                            veff, 1, 1.0, 0.0, 0.0, use_k);
+        return cheb_step<T>(c, c->nx, reinterpret_cast<const T*>(x), c->Nd, nullptr, 0, reinterpret_cast<T*>(y),
+                            c->Nd, Vl, 1, 1.0, 0.0, 0.0, use_k);
     };
     auto dot = [&](const double* x, const double* y, double* r) -> int {
         CUBLAS_TRY(cublasDdot(c->cublas, (int)Nv, x, 1, y, 1, r));  // Re<x,y> for interleaved complex too
@@ -746,6 +915,7 @@ int lanczos_impl(lynx_ctx* c, const double* veff, double tol, int max_iter, doub
         pmax = emax;
         ++j;
     }
+    LYNX_TRY(check_errflag(c));
     *eigmax = emax * 1.01;
     *eigmin = emin - 0.1;
     return LYNX_OK;
@@ -895,6 +1065,10 @@ int lynx_destroy(lynx_ctx* c) {
     c->info.release();
     c->io_psi.release();
     c->io_v.release();
+    c->vpad64.release();
+    c->vpad32.release();
+    c->errflag.release();
+    for (auto& b : c->nl_layout_bufs) b.release();
     if (c->cublas) cublasDestroy(c->cublas);
     if (c->cusolver) cusolverDnDestroy(c->cusolver);
     delete c;
@@ -939,6 +1113,11 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
     LYNX_TRY(activate(c));
     for (auto& b : c->nl_bufs) b.release();
     c->nl_bufs.clear();
+    for (auto& b : c->nl_layout_bufs) b.release();
+    c->nl_layout_bufs.clear();
+    c->nl_layouts.clear();
+    c->h_gpos.clear();
+    c->h_pt_grid.clear();
     c->nl = NLDev();
     c->has_nl = false;
     c->img_shift.clear();
@@ -1039,6 +1218,8 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
     LYNX_TRY(up(ent_img.data(), ent_img.size() * 4, (void**)&d.ent_img));
     LYNX_TRY(up(ent_loc.data(), ent_loc.size() * 4, (void**)&d.ent_loc));
     c->img_shift.assign(img_shift, img_shift + 3 * n_img);
+    c->h_gpos.assign(gpos, gpos + tot);
+    c->h_pt_grid = pt_grid;
     c->has_nl = true;
     return update_nl_phases(c);
 }
@@ -1061,7 +1242,10 @@ int lynx_hamiltonian_apply(lynx_ctx* c, const double* psi, const double* veff, d
     LYNX_TRY(activate(c));
     const long long l = ld > 0 ? ld : c->Nd;
     LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
-    return cheb_step<double>(c, psi, l, nullptr, 0, y, l, veff, ncol, 1.0, cs, 0.0, false);
+    const double* Vl = nullptr;
+    LYNX_TRY(veff_layout<double>(c, veff, c->nx, &Vl));
+    LYNX_TRY(cheb_step<double>(c, c->nx, psi, l, nullptr, 0, y, l, Vl, ncol, 1.0, cs, 0.0, false));
+    return check_errflag(c);
 }
 
 int lynx_hamiltonian_apply_kpt(lynx_ctx* c, const double* psi, const double* veff, double* y, int ncol, int ld,
@@ -1075,8 +1259,11 @@ int lynx_hamiltonian_apply_kpt(lynx_ctx* c, const double* psi, const double* vef
     LYNX_TRY(activate(c));
     const long long l = ld > 0 ? ld : c->Nd;
     LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
-    return cheb_step<double2>(c, reinterpret_cast<const double2*>(psi), l, nullptr, 0,
-                              reinterpret_cast<double2*>(y), l, veff, ncol, 1.0, cs, 0.0, true);
+    const double* Vl = nullptr;
+    LYNX_TRY(veff_layout<double>(c, veff, c->nx, &Vl));
+    LYNX_TRY(cheb_step<double2>(c, c->nx, reinterpret_cast<const double2*>(psi), l, nullptr, 0,
+                                reinterpret_cast<double2*>(y), l, Vl, ncol, 1.0, cs, 0.0, true));
+    return check_errflag(c);
 }
 
 int lynx_nonlocal_apply(lynx_ctx* c, const double* psi, double* hpsi, int ncol, int ld) {
@@ -1116,44 +1303,34 @@ static int filter_entry(lynx_ctx* c, const double* X, double* Y, const double* v
     LYNX_TRY(activate(c));
     const long long Nd = c->Nd, l = ld > 0 ? ld : Nd;
     LYNX_CHECK_ARG(l >= Nd, "ld < Nd");
-    const size_t esz = cplx ? 2 : 1;
+    long long ldb = 0;
+    int nxp = 0;
     if (precision == LYNX_PREC_FP64) {
-        const size_t blk = sizeof(double) * esz * (size_t)Nd * ncol;
-        for (int i = 0; i < 3; ++i) LYNX_TRY(c->wbuf[i].ensure(blk));
         if (cplx) {
-            double2* b[3] = {c->wbuf[0].as<double2>(), c->wbuf[1].as<double2>(), c->wbuf[2].as<double2>()};
-            double2* out = nullptr;
-            LYNX_TRY(filter_blocks<double2>(c, reinterpret_cast<const double2*>(X), l, b, veff, ncol, lc, emin, emax,
-                                            degree, true, &out));
-            LYNX_CUDA_TRY(cudaMemcpy2DAsync(Y, l * 16, out, Nd * 16, Nd * 16, ncol, cudaMemcpyDeviceToDevice, c->stream));
+            double2 *out = nullptr, *unused = nullptr;
+            LYNX_TRY(run_filter64<double2>(c, reinterpret_cast<const double2*>(X), l, veff, ncol, lc, emin, emax,
+                                           degree, true, false, &out, &unused, &ldb, &nxp));
+            LYNX_TRY(repack<double2, double2>(c, reinterpret_cast<double2*>(Y), c->nx, l, out, nxp, ldb, ncol));
         } else {
-            double* b[3] = {c->wbuf[0].as<double>(), c->wbuf[1].as<double>(), c->wbuf[2].as<double>()};
-            double* out = nullptr;
-            LYNX_TRY(filter_blocks<double>(c, X, l, b, veff, ncol, lc, emin, emax, degree, false, &out));
-            LYNX_CUDA_TRY(cudaMemcpy2DAsync(Y, l * 8, out, Nd * 8, Nd * 8, ncol, cudaMemcpyDeviceToDevice, c->stream));
+            double *out = nullptr, *unused = nullptr;
+            LYNX_TRY(run_filter64<double>(c, X, l, veff, ncol, lc, emin, emax, degree, false, false, &out, &unused,
+                                          &ldb, &nxp));
+            LYNX_TRY(repack<double, double>(c, Y, c->nx, l, out, nxp, ldb, ncol));
         }
     } else {
-        int st = LYNX_OK;
-        const float* v32 = veff_as<float>(c, veff, &st);
-        if (st) return st;
-        const size_t blk = sizeof(float) * esz * (size_t)Nd * ncol;
-        for (int i = 0; i < 4; ++i) LYNX_TRY(c->wbuf[i].ensure(blk));
         if (cplx) {
-            float2* X32 = c->wbuf[3].as<float2>();
-            LYNX_TRY(convert_cols<float2, double2>(X32, Nd, reinterpret_cast<const double2*>(X), l, Nd, ncol, c->stream));
-            float2* b[3] = {c->wbuf[0].as<float2>(), c->wbuf[1].as<float2>(), c->wbuf[2].as<float2>()};
-            float2* out = nullptr;
-            LYNX_TRY(filter_blocks<float2>(c, X32, Nd, b, v32, ncol, lc, emin, emax, degree, true, &out));
-            LYNX_TRY(convert_cols<double2, float2>(reinterpret_cast<double2*>(Y), l, out, Nd, Nd, ncol, c->stream));
+            float2 *out = nullptr, *unused = nullptr;
+            LYNX_TRY(run_filter32<float2, double2>(c, reinterpret_cast<const double2*>(X), l, veff, ncol, lc, emin,
+                                                   emax, degree, true, false, &out, &unused, &ldb, &nxp));
+            LYNX_TRY(repack<double2, float2>(c, reinterpret_cast<double2*>(Y), c->nx, l, out, nxp, ldb, ncol));
         } else {
-            float* X32 = c->wbuf[3].as<float>();
-            LYNX_TRY(convert_cols<float, double>(X32, Nd, X, l, Nd, ncol, c->stream));
-            float* b[3] = {c->wbuf[0].as<float>(), c->wbuf[1].as<float>(), c->wbuf[2].as<float>()};
-            float* out = nullptr;
-            LYNX_TRY(filter_blocks<float>(c, X32, Nd, b, v32, ncol, lc, emin, emax, degree, false, &out));
-            LYNX_TRY(convert_cols<double, float>(Y, l, out, Nd, Nd, ncol, c->stream));
+            float *out = nullptr, *unused = nullptr;
+            LYNX_TRY(run_filter32<float, double>(c, X, l, veff, ncol, lc, emin, emax, degree, false, false, &out,
+                                                 &unused, &ldb, &nxp));
+            LYNX_TRY(repack<double, float>(c, Y, c->nx, l, out, nxp, ldb, ncol));
         }
     }
+    LYNX_TRY(check_errflag(c));
     return LYNX_OK;
 }
 
@@ -1215,9 +1392,10 @@ int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precisi
         return LYNX_ERR_UNSUPPORTED;
     }
     LYNX_TRY(activate(c));
-    const long long Nd = c->Nd;
     const size_t esz = precision == LYNX_PREC_FP64 ? sizeof(double) : sizeof(float);
-    for (int i = 0; i < 3; ++i) LYNX_TRY(c->wbuf[i].ensure(esz * (size_t)Nd * ncol));
+    const int nxp = pipe_row_elems(c->nx, esz);
+    const long long ldb = (long long)nxp * c->ny * c->nz;
+    for (int i = 0; i < 3; ++i) LYNX_TRY(ensure_zeroed(c, c->wbuf[i], esz * (size_t)ldb * ncol));
     const bool nl = c->has_nl;
     if (!with_nonlocal) c->has_nl = false;
     cudaEvent_t e0, e1;
@@ -1225,16 +1403,18 @@ int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precisi
     cudaEventCreate(&e1);
     int st = LYNX_OK;
     const float* v32 = nullptr;
-    if (precision == LYNX_PREC_MIXED) v32 = veff_as<float>(c, veff, &st);
+    const double* v64 = nullptr;
+    if (precision == LYNX_PREC_MIXED) st = veff_layout<float>(c, veff, nxp, &v32);
+    else st = veff_layout<double>(c, veff, nxp, &v64);
     for (int r = -1; r < reps && st == LYNX_OK; ++r) {  // r = -1: untimed warm-up launch
         if (r == 0) cudaEventRecord(e0, c->stream);
         const int a = (r + 3) % 3, b = (r + 4) % 3, o = (r + 5) % 3;
         if (precision == LYNX_PREC_FP64)
-            st = cheb_step<double>(c, c->wbuf[a].as<double>(), Nd, c->wbuf[b].as<double>(), Nd,
-                                   c->wbuf[o].as<double>(), Nd, veff, ncol, 0.5, -0.1, -0.25, false);
+            st = cheb_step<double>(c, nxp, c->wbuf[a].as<double>(), ldb, c->wbuf[b].as<double>(), ldb,
+                                   c->wbuf[o].as<double>(), ldb, v64, ncol, 0.5, -0.1, -0.25, false);
         else
-            st = cheb_step<float>(c, c->wbuf[a].as<float>(), Nd, c->wbuf[b].as<float>(), Nd,
-                                  c->wbuf[o].as<float>(), Nd, v32, ncol, 0.5, -0.1, -0.25, false);
+            st = cheb_step<float>(c, nxp, c->wbuf[a].as<float>(), ldb, c->wbuf[b].as<float>(), ldb,
+                                  c->wbuf[o].as<float>(), ldb, v32, ncol, 0.5, -0.1, -0.25, false);
     }
     cudaEventRecord(e1, c->stream);
     cudaEventSynchronize(e1);
@@ -1245,6 +1425,7 @@ int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precisi
     c->has_nl = nl;
     if (st != LYNX_OK) return st;
     LYNX_CUDA_TRY(cudaGetLastError());
+    LYNX_TRY(check_errflag(c));
     *ms_per_step = ms / reps;
     return LYNX_OK;
 }

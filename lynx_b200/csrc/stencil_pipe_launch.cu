@@ -1,0 +1,159 @@
+// Launch-shape selection and template dispatch for the pipelined Chebyshev-step kernel.
+// LYNX_STENCIL_TYPES = 0: real (double, float); 1: complex (double2, float2).
+#include <algorithm>
+#include <cstdio>
+#include <type_traits>
+
+#include "kernels.h"
+#include "lynx_common.cuh"
+#include "stencil_pipe.cuh"
+
+namespace lynxb {
+
+namespace {
+
+template <typename T> struct PipeShape;
+// RX adjacent x points x RY rows per thread, launch-bound thread count.
+template <> struct PipeShape<float> { static constexpr int RX = 2, RY = 4; };
+template <> struct PipeShape<double> { static constexpr int RX = 2, RY = 2; };
+template <> struct PipeShape<float2> { static constexpr int RX = 1, RY = 4; };
+template <> struct PipeShape<double2> { static constexpr int RX = 1, RY = 2; };
+
+template <typename T, int R, bool XOLD>
+void launch_pipe(dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x, const T* xo, T* out,
+                 const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C, int* err) {
+    constexpr int RX = PipeShape<T>::RX, RY = PipeShape<T>::RY;
+    auto kern = cheb_pipe_kernel<T, R, RX, RY, XOLD>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<grid, nthr, smem, st>>>(x, xo, out, V, G, C, err);
+}
+
+}  // namespace
+
+template <typename T, typename S>
+int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out,
+                     long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl, const T* phr,
+                     int* err, cudaStream_t st) {
+    static_assert(std::is_same<S, typename ScalarOf<T>::type>::value, "scalar type mismatch");
+    constexpr int RX = PipeShape<T>::RX, RY = PipeShape<T>::RY;
+    const int R = g.R;
+    if (R < 1 || R > 8) {
+        set_error("FD half-width %d outside the supported range 1..8", R);
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    if (g.nx < R || g.ny < R || g.nz < R) {
+        set_error("grid %dx%dx%d smaller than the FD half-width %d", g.nx, g.ny, g.nz, R);
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    if (nxp < g.nx || (nxp * sizeof(S)) % 16 != 0 || (ldx * sizeof(T)) % 16 || (ldout * sizeof(T)) % 16 ||
+        (xold && (ldo * sizeof(T)) % 16)) {
+        set_error("pipelined stencil needs 16-byte aligned rows and columns");
+        return LYNX_ERR_BAD_ARG;
+    }
+    if (ncol <= 0) return LYNX_OK;
+    const int P2 = (g.nx + RX - 1) / RX;
+    if (P2 > kPipeMaxThreads) {
+        set_error("nx = %d too large for the pipelined stencil", g.nx);
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    int TYT = std::max(1, (192 + P2 / 2) / P2);
+    TYT = std::min(TYT, kPipeMaxThreads / P2);
+    TYT = std::min(TYT, (g.ny + RY - 1) / RY);
+    const int nthr = ((P2 * TYT + 31) / 32) * 32;
+    PipeGeom G;
+    G.nx = g.nx;
+    G.ny = g.ny;
+    G.nz = g.nz;
+    G.nxp = nxp;
+    const int q = (int)(16 / sizeof(T)) > 0 ? (int)(16 / sizeof(T)) : 1;
+    const int XOFF = (R % RX == 0) ? R : (R + RX - (R % RX));
+    G.GL = ((XOFF + q - 1) / q) * q;
+    {
+        const int rx_nx = ((g.nx + RX - 1) / RX) * RX;
+        int sp = std::max(G.GL + nxp, G.GL + rx_nx + XOFF + RX);
+        G.SP = ((sp + q - 1) / q) * q;
+    }
+    G.TYT = TYT;
+    G.TY = TYT * RY;
+    G.P2 = P2;
+    G.plane = (long long)nxp * g.ny;
+    G.ld_x = ldx;
+    G.ld_old = ldo;
+    G.ld_out = ldout;
+    const int nbands = (g.ny + G.TY - 1) / G.TY;
+    const long long base = (long long)nbands * ncol;
+    int nzch = (int)std::min<long long>((600 + base - 1) / base, std::max(1, g.nz / (4 * R)));
+    nzch = std::max(1, nzch);
+    G.zchunk = (g.nz + nzch - 1) / nzch;
+    nzch = (g.nz + G.zchunk - 1) / G.zchunk;
+    const bool xo = (xold != nullptr) && d != 0.0;
+    const size_t tile_b = (size_t)(G.TY + 2 * R) * G.SP * sizeof(T);
+    const size_t own_b = (size_t)G.TY * nxp * sizeof(T);
+    const size_t v_b = (size_t)G.TY * nxp * sizeof(S);
+    const size_t stage = ((tile_b + (xo ? own_b : 0) + v_b + 127) / 128) * 128;
+    const size_t smem = 128 + kPipeStages * stage;
+    if (smem > 227 * 1024) {
+        set_error("pipelined stencil stage of %zu bytes exceeds shared memory", smem);
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    if (ncol > 65535 || nzch > 65535) {
+        set_error("too many columns (%d) for one launch", ncol);
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    PipeCoef<T> C;
+    for (int p = 0; p <= 8; ++p) C.cx[p] = C.cy[p] = C.cz[p] = S(0);
+    for (int p = 1; p <= R; ++p) {
+        C.cx[p] = (S)(-0.5 * a * g.D2x[p]);
+        C.cy[p] = (S)(-0.5 * a * g.D2y[p]);
+        C.cz[p] = (S)(-0.5 * a * g.D2z[p]);
+    }
+    C.diag = (S)(-0.5 * a * (g.D2x[0] + g.D2y[0] + g.D2z[0]) + b);
+    C.a = (S)a;
+    C.d = (S)d;
+    for (int k = 0; k < 3; ++k) {
+        C.phl[k] = phl[k];
+        C.phr[k] = phr[k];
+    }
+    dim3 grid(nbands, ncol, nzch);
+#define LYNX_PIPE_CASE(RR)                                                                       \
+    case RR:                                                                                     \
+        if (xo) launch_pipe<T, RR, true>(grid, nthr, smem, st, x, xold, out, V, G, C, err);       \
+        else launch_pipe<T, RR, false>(grid, nthr, smem, st, x, xold, out, V, G, C, err);         \
+        break;
+    switch (R) {
+        LYNX_PIPE_CASE(1)
+        LYNX_PIPE_CASE(2)
+        LYNX_PIPE_CASE(3)
+        LYNX_PIPE_CASE(4)
+        LYNX_PIPE_CASE(5)
+        LYNX_PIPE_CASE(6)
+        LYNX_PIPE_CASE(7)
+        LYNX_PIPE_CASE(8)
+    }
+#undef LYNX_PIPE_CASE
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("pipelined stencil launch failed: %s", cudaGetErrorString(e));
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+#if LYNX_STENCIL_TYPES == 0
+template int launch_cheb_pipe<double, double>(const StencilGeom&, int, const double*, long long, const double*,
+                                              long long, double*, long long, const double*, int, double, double,
+                                              double, const double*, const double*, int*, cudaStream_t);
+template int launch_cheb_pipe<float, float>(const StencilGeom&, int, const float*, long long, const float*,
+                                            long long, float*, long long, const float*, int, double, double, double,
+                                            const float*, const float*, int*, cudaStream_t);
+#else
+template int launch_cheb_pipe<double2, double>(const StencilGeom&, int, const double2*, long long, const double2*,
+                                               long long, double2*, long long, const double*, int, double, double,
+                                               double, const double2*, const double2*, int*, cudaStream_t);
+template int launch_cheb_pipe<float2, float>(const StencilGeom&, int, const float2*, long long, const float2*,
+                                             long long, float2*, long long, const float*, int, double, double,
+                                             double, const float2*, const float2*, int*, cudaStream_t);
+#endif
+
+}  // namespace lynxb
