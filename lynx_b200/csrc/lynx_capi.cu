@@ -363,6 +363,10 @@ template <> struct Real<float2> { using type = float; };
 
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
+// The pipelined stencil pairs adjacent x points for real data, so it needs an even nx;
+// other grids keep unpadded rows and run the register-window kernel.
+template <typename T> bool pipe_capable(int nx) { return ScalarOf<T>::cplx || nx % 2 == 0; }
+
 // Grows a work buffer; new storage is zeroed so that the padding elements of padded
 // row layouts read as zero.
 int ensure_zeroed(lynx_ctx* c, DevBuf& b, size_t bytes) {
@@ -473,7 +477,7 @@ int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, lo
     using S = typename Real<T>::type;
     T phl[3], phr[3];
     ghost_phases<T>(c, use_k, phl, phr);
-    const bool pipe_ok = (nxp * sizeof(S)) % 16 == 0 && (ldx * sizeof(T)) % 16 == 0 &&
+    const bool pipe_ok = pipe_capable<T>(c->nx) && (nxp * sizeof(S)) % 16 == 0 && (ldx * sizeof(T)) % 16 == 0 &&
                          (ldout * sizeof(T)) % 16 == 0 && (!xold || (ldo * sizeof(T)) % 16 == 0) && aligned16(x) &&
                          aligned16(out) && (!xold || aligned16(xold)) && aligned16(V);
     if (!pipe_ok && nxp != c->nx) {
@@ -539,7 +543,7 @@ template <typename T64>
 int run_filter64(lynx_ctx* c, const T64* X, long long ldX, const double* veff, int N, double lc, double emin,
                  double emax, int degree, bool use_k, bool want_hy, T64** Y, T64** HY, long long* ldb, int* nxp) {
     using S = typename Real<T64>::type;
-    *nxp = pipe_row_elems(c->nx, sizeof(S));
+    *nxp = pipe_capable<T64>(c->nx) ? pipe_row_elems(c->nx, sizeof(S)) : c->nx;
     *ldb = (long long)(*nxp) * c->ny * c->nz;
     const size_t blk = sizeof(T64) * (size_t)(*ldb) * N;
     const bool direct = (*nxp == c->nx) && (ldX * sizeof(T64)) % 16 == 0 && aligned16(X);
@@ -567,7 +571,7 @@ template <typename T32, typename T64>
 int run_filter32(lynx_ctx* c, const T64* X, long long ldX, const double* veff, int N, double lc, double emin,
                  double emax, int degree, bool use_k, bool want_hy, T32** Y, T32** HY, long long* ldb, int* nxp) {
     using S = typename Real<T32>::type;
-    *nxp = pipe_row_elems(c->nx, sizeof(S));
+    *nxp = pipe_capable<T32>(c->nx) ? pipe_row_elems(c->nx, sizeof(S)) : c->nx;
     *ldb = (long long)(*nxp) * c->ny * c->nz;
     const size_t blk = sizeof(T32) * (size_t)(*ldb) * N;
     for (int i = 0; i < 4; ++i) LYNX_TRY(ensure_zeroed(c, c->wbuf[i], blk));
@@ -1393,7 +1397,7 @@ int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precisi
     }
     LYNX_TRY(activate(c));
     const size_t esz = precision == LYNX_PREC_FP64 ? sizeof(double) : sizeof(float);
-    const int nxp = pipe_row_elems(c->nx, esz);
+    const int nxp = (c->nx % 2 == 0) ? pipe_row_elems(c->nx, esz) : c->nx;
     const long long ldb = (long long)nxp * c->ny * c->nz;
     for (int i = 0; i < 3; ++i) LYNX_TRY(ensure_zeroed(c, c->wbuf[i], esz * (size_t)ldb * ncol));
     const bool nl = c->has_nl;

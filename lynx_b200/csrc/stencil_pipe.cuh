@@ -29,13 +29,13 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 #include "stencil.cuh"
 
 namespace lynxb {
 
-constexpr int kPipeStages = 3;        // P + 1
-constexpr int kPipeMaxThreads = 384;
+constexpr int kPipeMaxThreads = 352;
 constexpr long long kSpinLimit = 1LL << 22;  // bounded mbarrier waits
 
 struct PipeGeom {
@@ -108,76 +108,141 @@ __device__ __forceinline__ void fence_mbar_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Pipelined kernel.  RX adjacent x points and RY adjacent rows per thread.
-template <typename T, int R, int RX, int RY, bool XOLD>
-__global__ void __launch_bounds__(kPipeMaxThreads)
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Warp-specialised pipelined kernel.  The last warp of the CTA is the producer: it keeps
+// NS stages of the shared-memory ring in flight with bulk copies (the band's rows plus R
+// halo rows on each side as one contiguous copy, two where the band meets the y boundary;
+// xold and Veff rows; and, in a separate DW-stage ring, the rows of the plane entering the
+// z-window).  The other warps are consumers: each thread computes RX adjacent x points on
+// RY adjacent rows.  Staged rows carry no ghost columns: a consumer reads its x neighbours
+// through column offsets wrapped once at start-up, and PHASED instantiations (Bloch phases,
+// Dirichlet zeros) multiply wrapped neighbours in registers.  Per stage two mbarriers:
+// full (copies landed, tx-counted) and empty (every consumer warp done reading).
+template <typename T, int R, int RX, int RY, bool XOLD, int NS, bool PHASED>
+__global__ void __launch_bounds__(kPipeMaxThreads, 1)
     cheb_pipe_kernel(const T* __restrict__ x, const T* __restrict__ xold, T* __restrict__ out,
                      const typename ScalarOf<T>::type* __restrict__ V, const PipeGeom G, const PipeCoef<T> C,
                      int* __restrict__ err) {
     using S = typename ScalarOf<T>::type;
     using VT = typename VecOf<T, RX>::type;
     constexpr int W = 2 * R + 1;
-    constexpr int NS = kPipeStages;
-    constexpr int P = NS - 1;
+    constexpr int DW = 4;  // window ring depth
+    static_assert((2 * NS + 2 * DW) * 8 <= 256, "ring size out of range");
     // x-neighbour vector loads: first element index rounded down to a multiple of RX
     constexpr int XOFF = (R % RX == 0) ? R : (R + RX - (R % RX));  // XOFF >= R, XOFF % RX == 0
     constexpr int NXV = (XOFF + R + RX + RX - 1) / RX;            // vectors covering x-XOFF .. x+RX-1+R
 
     extern __shared__ __align__(128) unsigned char smpipe[];
     const int tid = threadIdx.x;
-    const int nthr = blockDim.x;
+    const int NC = blockDim.x - 32;  // consumer threads (a multiple of 32)
     const int nx = G.nx, ny = G.ny, nz = G.nz;
+    const int nxp = G.nxp;
     const int y0 = blockIdx.x * G.TY;
     const int TYv = min(G.TY, ny - y0);
     const int z0 = blockIdx.z * G.zchunk;
     const int z1 = min(nz, z0 + G.zchunk);
+    const int nplanes = z1 - z0;
     const long long col = blockIdx.y;
     const T* __restrict__ xc = x + col * G.ld_x;
     const T* __restrict__ xoc = XOLD ? xold + col * G.ld_old : nullptr;
     T* __restrict__ oc = out + col * G.ld_out;
 
-    // Shared-memory carve-up: [mbarriers][stage 0][stage 1]...; a stage holds the staged
-    // tile ((TY + 2R) rows of pitch SP), then xold rows and Veff rows (TY x nxp each).
-    const int tile_elems = (G.TY + 2 * R) * G.SP;
-    const int own_elems = G.TY * G.nxp;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smpipe);
-    T* stage0 = reinterpret_cast<T*>(smpipe + 128);
+    // Shared memory: [mbarriers][NS tile stages][DW window stages]; a tile stage holds
+    // (TY + 2R) rows of the plane (pitch nxp), then xold and Veff on the band's rows.
+    const int tile_elems = (G.TY + 2 * R) * nxp;
+    const int own_elems = G.TY * nxp;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smpipe);
+    uint64_t* empty = full + NS;
+    uint64_t* wfull = empty + NS;
+    uint64_t* wempty = wfull + DW;
+    T* stage0 = reinterpret_cast<T*>(smpipe + 256);
     const int stage_bytes_T = (tile_elems + (XOLD ? own_elems : 0)) * (int)sizeof(T);
     const int stage_stride = ((stage_bytes_T + own_elems * (int)sizeof(S) + 127) / 128) * 128;
-    auto tile_of = [&](int s) { return reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(stage0) + s * stage_stride); };
-    auto xold_of = [&](int s) { return tile_of(s) + tile_elems; };
-    auto veff_of = [&](int s) {
-        return reinterpret_cast<S*>(reinterpret_cast<unsigned char*>(tile_of(s)) + stage_bytes_T);
+    const int wstage_stride = ((own_elems * (int)sizeof(T) + 127) / 128) * 128;
+    auto tile_of = [&](int st) {
+        return reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(stage0) + st * stage_stride);
+    };
+    auto xold_of = [&](int st) { return tile_of(st) + tile_elems; };
+    auto veff_of = [&](int st) {
+        return reinterpret_cast<S*>(reinterpret_cast<unsigned char*>(tile_of(st)) + stage_bytes_T);
+    };
+    auto wstage_of = [&](int st) {
+        return reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(stage0) + NS * stage_stride + st * wstage_stride);
     };
 
     if (tid == 0) {
-        for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
+        for (int st = 0; st < NS; ++st) {
+            mbar_init(&full[st], 1);
+            mbar_init(&empty[st], NC / 32);
+        }
+        for (int st = 0; st < DW; ++st) {
+            mbar_init(&wfull[st], 1);
+            mbar_init(&wempty[st], NC / 32);
+        }
         fence_mbar_init();
     }
     __syncthreads();
 
-    // Producer: all copies of plane z into stage s (elected thread 0).
-    auto issue = [&](int z, int s) {
-        T* tile = tile_of(s);
-        const uint32_t rowb = (uint32_t)(G.nxp * sizeof(T));
-        const uint32_t ownb = (uint32_t)(TYv * G.nxp * sizeof(T));
-        const uint32_t vb = (uint32_t)(TYv * G.nxp * sizeof(S));
-        const uint32_t total = (uint32_t)(TYv + 2 * R) * rowb + (XOLD ? ownb : 0u) + vb;
-        fence_proxy_async_smem();
-        mbar_expect_tx(&bars[s], total);
-        const T* plane = xc + (long long)z * G.plane;
-        for (int t = 0; t < TYv + 2 * R; ++t) {
-            int gy = y0 - R + t;
-            gy += (gy < 0) ? ny : 0;
-            gy -= (gy >= ny) ? ny : 0;
-            bulk_g2s(tile + t * G.SP + G.GL, plane + (long long)gy * G.nxp, rowb, &bars[s]);
+    if (tid >= NC) {
+        // ------------------------------ producer warp ------------------------------
+        if (tid != NC) return;  // one elected thread issues every copy
+        const uint32_t rowb = (uint32_t)(nxp * sizeof(T));
+        const uint32_t ownb = (uint32_t)(TYv * nxp * sizeof(T));
+        const uint32_t vb = (uint32_t)(TYv * nxp * sizeof(S));
+        const int nrows = TYv + 2 * R;
+        const uint32_t total = (uint32_t)nrows * rowb + (XOLD ? ownb : 0u) + vb;
+        // rows y0-R .. y0+TYv+R-1 as up to three contiguous runs of global rows (y wraps)
+        int run_t[3], run_y[3], run_n[3], nruns = 0;
+        {
+            int t = 0;
+            while (t < nrows) {
+                int gy = y0 - R + t;
+                gy += (gy < 0) ? ny : 0;
+                gy -= (gy >= ny) ? ny : 0;
+                const int n = min(nrows - t, ny - gy);
+                run_t[nruns] = t;
+                run_y[nruns] = gy;
+                run_n[nruns] = n;
+                ++nruns;
+                t += n;
+            }
         }
-        const long long own0 = (long long)z * G.plane + (long long)y0 * G.nxp;
-        if (XOLD) bulk_g2s(xold_of(s), xoc + own0, ownb, &bars[s]);
-        bulk_g2s(veff_of(s), V + (long long)z * G.plane + (long long)y0 * G.nxp, vb, &bars[s]);
-    };
+        for (int i = 0; i < nplanes; ++i) {
+            const int z = z0 + i;
+            const int st = i % NS, k = i / NS;
+            if (k > 0 && !mbar_wait(&empty[st], (uint32_t)((k - 1) & 1))) {
+                atomicExch(err, 1);
+                return;
+            }
+            mbar_expect_tx(&full[st], total);
+            T* tile = tile_of(st);
+            const T* plane = xc + (long long)z * G.plane;
+            for (int q = 0; q < nruns; ++q)
+                bulk_g2s(tile + run_t[q] * nxp, plane + (long long)run_y[q] * nxp, run_n[q] * rowb, &full[st]);
+            const long long own0 = (long long)z * G.plane + (long long)y0 * nxp;
+            if (XOLD) bulk_g2s(xold_of(st), xoc + own0, ownb, &full[st]);
+            bulk_g2s(veff_of(st), V + own0, vb, &full[st]);
+            // rows of the plane that enters the consumers' z-window after iteration i
+            if (i + 1 < nplanes) {
+                const int wst = i % DW, wk = i / DW;
+                if (wk > 0 && !mbar_wait(&wempty[wst], (uint32_t)((wk - 1) & 1))) {
+                    atomicExch(err, 1);
+                    return;
+                }
+                int zw = z + R + 1;
+                zw -= (zw >= nz) ? nz : 0;
+                mbar_expect_tx(&wfull[wst], ownb);
+                bulk_g2s(wstage_of(wst), xc + (long long)zw * G.plane + (long long)y0 * nxp, ownb, &wfull[wst]);
+            }
+        }
+        return;
+    }
 
-    // Thread block of points.
+    // ------------------------------ consumer warps ------------------------------
+    const int lane = tid & 31;
     const int px = tid % G.P2;
     const int ty = tid / G.P2;
     const int xb = px * RX;  // first x of the block
@@ -189,6 +254,34 @@ __global__ void __launch_bounds__(kPipeMaxThreads)
         own[r] = (ty < G.TYT) && (yl[r] < TYv);
     }
     const T zero = vzero(T());
+    // x-neighbour vectors: start columns wrapped into [0, nx) (nx is a multiple of RX, so a
+    // vector never straddles the boundary); bit 2k / 2k+1 of xwrap: vector k wrapped left/right.
+    int xcol[NXV];
+    unsigned xwrap = 0;
+#pragma unroll
+    for (int k = 0; k < NXV; ++k) {
+        int c = xb - XOFF + k * RX;
+        if (c < 0) {
+            c += nx;
+            xwrap |= 1u << (2 * k);
+        } else if (c >= nx) {
+            c -= nx;
+            xwrap |= 2u << (2 * k);
+        }
+        xcol[k] = c;
+    }
+    // y neighbours row R + yl +- p (staged rows); bit (r*2R + 2(p-1)) / +1: the row above / below
+    // was copied across the y boundary (top rows wrap left, bottom rows wrap right).
+    unsigned long long ywrap = 0;
+    if (PHASED) {
+#pragma unroll
+        for (int r = 0; r < RY; ++r)
+#pragma unroll
+            for (int p = 1; p <= R; ++p) {
+                if (y0 + yl[r] + p >= ny) ywrap |= 1ull << (r * 2 * R + 2 * (p - 1));
+                if (y0 + yl[r] - p < 0) ywrap |= 2ull << (r * 2 * R + 2 * (p - 1));
+            }
+    }
 
     auto load_own_plane = [&](int zz, VT* v) {
         T mul = C.phl[2];
@@ -201,155 +294,199 @@ __global__ void __launch_bounds__(kPipeMaxThreads)
             mul = C.phr[2];
             wrapped = true;
         }
-        const T* base = xc + (long long)zz * G.plane + (long long)y0 * G.nxp + xb;
+        const T* base = xc + (long long)zz * G.plane + (long long)y0 * nxp + xb;
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
             VT t;
             if (own[r]) {
-                t = *reinterpret_cast<const VT*>(base + (long long)yl[r] * G.nxp);
+                t = *reinterpret_cast<const VT*>(base + (long long)yl[r] * nxp);
             } else {
                 T* tp = reinterpret_cast<T*>(&t);
 #pragma unroll
-                for (int i = 0; i < RX; ++i) tp[i] = zero;
+                for (int u = 0; u < RX; ++u) tp[u] = zero;
             }
             if (wrapped) {
                 T* tp = reinterpret_cast<T*>(&t);
 #pragma unroll
-                for (int i = 0; i < RX; ++i) tp[i] = pmul(tp[i], mul);
+                for (int u = 0; u < RX; ++u) tp[u] = pmul(tp[u], mul);
             }
             v[r] = t;
         }
     };
 
-    // Prologue: copies for the first P planes, window for the first plane, two planes of
-    // window prefetch.
-    if (tid == 0) {
-        for (int i = 0; i < P; ++i)
-            if (z0 + i < z1) issue(z0 + i, i);
+    // y neighbours of the thread's rows: staged rows R + yl[0] + q, q in [-R, RY-1+R].
+    // PHASED: bit (q+R) of ywrap_l / ywrap_r: that row was copied across the lower / upper y boundary.
+    unsigned ywrap_l = 0, ywrap_r = 0;
+    if (PHASED) {
+#pragma unroll
+        for (int q = -R; q < RY + R; ++q) {
+            const int gy = y0 + yl[0] + q;
+            if (gy < 0) ywrap_l |= 1u << (q + R);
+            else if (gy >= ny) ywrap_r |= 1u << (q + R);
+        }
     }
-    VT w[W][RY];
+
+    // z-window: 2R+2 slots so that two planes are marched per loop trip (slot j+k holds
+    // plane z-R+k for the plane z handled at sub-step j); sliding by two halves the moves.
+    VT w[W + 1][RY];
 #pragma unroll
     for (int k = 0; k < W; ++k) load_own_plane(z0 - R + k, w[k]);
-    VT pf0[RY], pf1[RY];
-    load_own_plane(z0 + R + 1, pf0);
-    load_own_plane(z0 + R + 2, pf1);
 
-    const T phl_x = C.phl[0], phr_x = C.phr[0];
-    const T phl_y = C.phl[1], phr_y = C.phr[1];
-    const bool wrap_top = (y0 - R) < 0;
-    const bool wrap_bot = (y0 + TYv + R) > ny;
-    const int ghost_rows = TYv + 2 * R;
-
-    for (int z = z0; z < z1; ++z) {
-        const int it = z - z0;
-        const int s = it % NS;
-        __syncthreads();  // S1: every thread is done with iteration it-1 (stage (it+P) % NS is free)
-        if (tid == 0 && z + P < z1) issue(z + P, (it + P) % NS);
-        // Wait for plane z.
-        bool ok = mbar_wait(&bars[s], (uint32_t)((it / NS) & 1));
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) atomicExch(err, 1);
-            return;
-        }
-        T* tile = tile_of(s);
-        // Bloch phase / Dirichlet zero on y-wrapped halo rows (rows copied from the other side).
-        if (ScalarOf<T>::cplx || wrap_top || wrap_bot) {
-            if (wrap_top || wrap_bot) {
-                for (int e = tid; e < 2 * R * nx; e += nthr) {
-                    const int hr = e / nx, hx = e - (e / nx) * nx;
-                    const int t = (hr < R) ? hr : (TYv + hr);
-                    const int gy = y0 - R + t;
-                    if (gy < 0) tile[t * G.SP + G.GL + hx] = pmul(tile[t * G.SP + G.GL + hx], phl_y);
-                    else if (gy >= ny) tile[t * G.SP + G.GL + hx] = pmul(tile[t * G.SP + G.GL + hx], phr_y);
+    // Entering plane of the window (plane z+R+1 after sub-step i), from the window ring.
+    auto window_entry = [&](int i, int z, VT* dst) -> bool {
+        const int wst = i % DW;
+        if (!mbar_wait(&wfull[wst], (uint32_t)((i / DW) & 1))) return false;
+        const T* wsrc = wstage_of(wst);
+        const bool wrapped = (z + R + 1) >= nz;
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+            VT t;
+            if (own[r]) {
+                t = *reinterpret_cast<const VT*>(wsrc + yl[r] * nxp + xb);
+                if (wrapped) {
+                    T* tp = reinterpret_cast<T*>(&t);
+#pragma unroll
+                    for (int u = 0; u < RX; ++u) tp[u] = pmul(tp[u], C.phr[2]);
                 }
-                __syncthreads();
+            } else {
+                T* tp = reinterpret_cast<T*>(&t);
+#pragma unroll
+                for (int u = 0; u < RX; ++u) tp[u] = zero;
+            }
+            dst[r] = t;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&wempty[wst]);
+        return true;
+    };
+
+    // One plane with the window starting at slot J.
+    auto plane_step = [&](auto Jc, int i) -> bool {
+        constexpr int J = decltype(Jc)::value;
+        const int z = z0 + i;
+        const int st = i % NS;
+        if (!mbar_wait(&full[st], (uint32_t)((i / NS) & 1))) return false;
+        const T* tile = tile_of(st);
+        const T* xo_s = XOLD ? xold_of(st) : nullptr;
+        const S* v_s = veff_of(st);
+        T acc[RY][RX];
+        // centre, z neighbours
+#pragma unroll
+        for (int r = 0; r < RY; ++r) {
+            const T* wc = reinterpret_cast<const T*>(&w[J + R][r]);
+#pragma unroll
+            for (int u = 0; u < RX; ++u) acc[r][u] = vscale(C.diag, wc[u]);
+#pragma unroll
+            for (int p = 1; p <= R; ++p) {
+                const T* a_ = reinterpret_cast<const T*>(&w[J + R + p][r]);
+                const T* b_ = reinterpret_cast<const T*>(&w[J + R - p][r]);
+#pragma unroll
+                for (int u = 0; u < RX; ++u) acc[r][u] = fmac(acc[r][u], C.cz[p], vadd(a_[u], b_[u]));
             }
         }
-        // x-ghost columns: left ghost x' = -p holds x(nx - p) * phl, right ghost x' = nx + p
-        // holds x(p) * phr.
-        for (int e = tid; e < ghost_rows * 2 * R; e += nthr) {
-            const int t = e / (2 * R);
-            const int g = e - t * (2 * R);
-            T* row = tile + t * G.SP + G.GL;
-            if (g < R) row[-R + g] = pmul(row[nx - R + g], phl_x);
-            else row[nx + (g - R)] = pmul(row[g - R], phr_x);
+        // y neighbours: each staged row is read once and feeds every row within R of it
+        {
+            const T* tcol = tile + (R + yl[0]) * nxp + xb;
+#pragma unroll
+            for (int q = -R; q < RY + R; ++q) {
+                VT v = *reinterpret_cast<const VT*>(tcol + q * nxp);
+                T* ve = reinterpret_cast<T*>(&v);
+                if (PHASED) {
+                    if (ywrap_l & (1u << (q + R))) {
+#pragma unroll
+                        for (int u = 0; u < RX; ++u) ve[u] = pmul(ve[u], C.phl[1]);
+                    } else if (ywrap_r & (1u << (q + R))) {
+#pragma unroll
+                        for (int u = 0; u < RX; ++u) ve[u] = pmul(ve[u], C.phr[1]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < RY; ++r) {
+                    const int d = (q > r) ? q - r : r - q;
+                    if (d >= 1 && d <= R) {
+#pragma unroll
+                        for (int u = 0; u < RX; ++u) acc[r][u] = fmac(acc[r][u], C.cy[d], ve[u]);
+                    }
+                }
+            }
         }
-        __syncthreads();  // S2: plane z staged with ghosts
-
-        // Compute the RX x RY block of plane z.
-        const T* xo_s = XOLD ? xold_of(s) : nullptr;
-        const S* v_s = veff_of(s);
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
             if (!own[r]) continue;
-            const int row = R + yl[r];
-            const T* trow = tile + row * G.SP + G.GL + xb;
-            T acc[RX];
-            const T* wc = reinterpret_cast<const T*>(&w[R][r]);
-#pragma unroll
-            for (int i = 0; i < RX; ++i) acc[i] = vscale(C.diag, wc[i]);
-            // x neighbours: vectors covering x-XOFF .. x+RX-1+R
+            const T* trow = tile + (R + yl[r]) * nxp;
+            // x neighbours
             {
                 T xv[NXV * RX];
 #pragma unroll
-                for (int k = 0; k < NXV; ++k)
-                    *reinterpret_cast<VT*>(&xv[k * RX]) = *reinterpret_cast<const VT*>(trow - XOFF + k * RX);
+                for (int k = 0; k < NXV; ++k) {
+                    VT t = *reinterpret_cast<const VT*>(trow + xcol[k]);
+                    if (PHASED) {
+                        T* tp = reinterpret_cast<T*>(&t);
+                        if (xwrap & (1u << (2 * k))) {
 #pragma unroll
-                for (int i = 0; i < RX; ++i)
+                            for (int u = 0; u < RX; ++u) tp[u] = pmul(tp[u], C.phl[0]);
+                        } else if (xwrap & (2u << (2 * k))) {
+#pragma unroll
+                            for (int u = 0; u < RX; ++u) tp[u] = pmul(tp[u], C.phr[0]);
+                        }
+                    }
+                    *reinterpret_cast<VT*>(&xv[k * RX]) = t;
+                }
+#pragma unroll
+                for (int u = 0; u < RX; ++u)
 #pragma unroll
                     for (int p = 1; p <= R; ++p)
-                        acc[i] = fmac(acc[i], C.cx[p], vadd(xv[XOFF + i + p], xv[XOFF + i - p]));
+                        acc[r][u] = fmac(acc[r][u], C.cx[p], vadd(xv[XOFF + u + p], xv[XOFF + u - p]));
             }
-            // y neighbours
+            const int so = yl[r] * nxp + xb;
+            const T* wc = reinterpret_cast<const T*>(&w[J + R][r]);
+            {
+                S vv[RX];
+                if constexpr (RX == 2) {
+                    using SV = typename VecOf<S, 2>::type;
+                    *reinterpret_cast<SV*>(vv) = *reinterpret_cast<const SV*>(v_s + so);
+                } else {
+                    vv[0] = v_s[so];
+                }
+                VT xo_v;
+                if (XOLD) xo_v = *reinterpret_cast<const VT*>(xo_s + so);
+                const T* xo_e = reinterpret_cast<const T*>(&xo_v);
 #pragma unroll
-            for (int p = 1; p <= R; ++p) {
-                const VT up = *reinterpret_cast<const VT*>(trow + p * G.SP);
-                const VT dn = *reinterpret_cast<const VT*>(trow - p * G.SP);
-                const T* u = reinterpret_cast<const T*>(&up);
-                const T* dd = reinterpret_cast<const T*>(&dn);
-#pragma unroll
-                for (int i = 0; i < RX; ++i) acc[i] = fmac(acc[i], C.cy[p], vadd(u[i], dd[i]));
+                for (int u = 0; u < RX; ++u) {
+                    acc[r][u] = fmac(acc[r][u], C.a * vv[u], wc[u]);
+                    if (XOLD) acc[r][u] = fmac(acc[r][u], C.d, xo_e[u]);
+                }
             }
-            // z neighbours
+            T* op = oc + (long long)z * G.plane + (long long)(y0 + yl[r]) * nxp + xb;
+            VT o;
+            T* opv = reinterpret_cast<T*>(&o);
 #pragma unroll
-            for (int p = 1; p <= R; ++p) {
-                const T* u = reinterpret_cast<const T*>(&w[R + p][r]);
-                const T* dd = reinterpret_cast<const T*>(&w[R - p][r]);
-#pragma unroll
-                for (int i = 0; i < RX; ++i) acc[i] = fmac(acc[i], C.cz[p], vadd(u[i], dd[i]));
-            }
-            const int so = yl[r] * G.nxp + xb;
-#pragma unroll
-            for (int i = 0; i < RX; ++i) {
-                acc[i] = fmac(acc[i], C.a * v_s[so + i], wc[i]);
-                if (XOLD) acc[i] = fmac(acc[i], C.d, xo_s[so + i]);
-            }
-            T* op = oc + (long long)z * G.plane + (long long)(y0 + yl[r]) * G.nxp + xb;
-            if (xb + RX <= nx) {
-                VT o;
-                T* opv = reinterpret_cast<T*>(&o);
-#pragma unroll
-                for (int i = 0; i < RX; ++i) opv[i] = acc[i];
-                *reinterpret_cast<VT*>(op) = o;
-            } else {
-#pragma unroll
-                for (int i = 0; i < RX; ++i)
-                    if (xb + i < nx) op[i] = acc[i];
-            }
+            for (int u = 0; u < RX; ++u) opv[u] = acc[r][u];
+            *reinterpret_cast<VT*>(op) = o;
         }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[st]);
+        return true;
+    };
 
-        // Slide the window and the prefetch.
+    bool ok = true;
+    for (int i = 0; i < nplanes && ok; i += 2) {
+        // sub-step 0: plane i, window slots 0..2R
+        ok = plane_step(std::integral_constant<int, 0>{}, i);
+        if (!ok || i + 1 >= nplanes) break;
+        ok = window_entry(i, z0 + i, w[W]);  // plane i+R+1 -> slot 2R+1
+        if (!ok) break;
+        // sub-step 1: plane i+1, window slots 1..2R+1
+        ok = plane_step(std::integral_constant<int, 1>{}, i + 1);
+        if (!ok || i + 2 >= nplanes) break;
+        // slide by two and bring in plane i+R+2
 #pragma unroll
         for (int k = 0; k < W - 1; ++k)
 #pragma unroll
-            for (int r = 0; r < RY; ++r) w[k][r] = w[k + 1][r];
-#pragma unroll
-        for (int r = 0; r < RY; ++r) {
-            w[W - 1][r] = pf0[r];
-            pf0[r] = pf1[r];
-        }
-        if (z + 1 < z1) load_own_plane(z + R + 3, pf1);
+            for (int r = 0; r < RY; ++r) w[k][r] = w[k + 2][r];
+        ok = window_entry(i + 1, z0 + i + 1, w[W - 1]);
     }
+    if (!ok && lane == 0) atomicExch(err, 1);
 }
 
 }  // namespace lynxb

@@ -19,13 +19,23 @@ template <> struct PipeShape<double> { static constexpr int RX = 2, RY = 2; };
 template <> struct PipeShape<float2> { static constexpr int RX = 1, RY = 4; };
 template <> struct PipeShape<double2> { static constexpr int RX = 1, RY = 2; };
 
-template <typename T, int R, bool XOLD>
-void launch_pipe(dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x, const T* xo, T* out,
-                 const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C, int* err) {
+template <typename T, int R, bool XOLD, bool PH>
+void launch_pipe_ph(int ns, dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x, const T* xo, T* out,
+                    const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C, int* err) {
     constexpr int RX = PipeShape<T>::RX, RY = PipeShape<T>::RY;
-    auto kern = cheb_pipe_kernel<T, R, RX, RY, XOLD>;
+    auto kern = ns >= 5 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 5, PH>
+               : (ns == 4 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 4, PH> : cheb_pipe_kernel<T, R, RX, RY, XOLD, 3, PH>);
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     kern<<<grid, nthr, smem, st>>>(x, xo, out, V, G, C, err);
+}
+
+// Real data with periodic boundaries needs no phase on wrapped neighbours; complex data and
+// Dirichlet boundaries use the PHASED instantiation.
+template <typename T, int R, bool XOLD>
+void launch_pipe(int ns, bool phased, dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x, const T* xo,
+                 T* out, const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C, int* err) {
+    if (ScalarOf<T>::cplx || phased) launch_pipe_ph<T, R, XOLD, true>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err);
+    else launch_pipe_ph<T, R, XOLD, false>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err);
 }
 
 }  // namespace
@@ -50,29 +60,33 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
         set_error("pipelined stencil needs 16-byte aligned rows and columns");
         return LYNX_ERR_BAD_ARG;
     }
+    if (g.nx % RX != 0) {
+        set_error("pipelined stencil needs nx to be a multiple of %d", RX);
+        return LYNX_ERR_UNSUPPORTED;
+    }
     if (ncol <= 0) return LYNX_OK;
-    const int P2 = (g.nx + RX - 1) / RX;
-    if (P2 > kPipeMaxThreads) {
+    const int P2 = g.nx / RX;
+    if (P2 > kPipeMaxThreads - 32) {
         set_error("nx = %d too large for the pipelined stencil", g.nx);
         return LYNX_ERR_UNSUPPORTED;
     }
-    int TYT = std::max(1, (192 + P2 / 2) / P2);
-    TYT = std::min(TYT, kPipeMaxThreads / P2);
+    // One CTA per SM: ~288 consumer threads (whole x-rows per thread row), bands balanced over ny.
+    int TYT = std::max(1, (288 + P2 / 2) / P2);
+    TYT = std::min(TYT, (kPipeMaxThreads - 32) / P2);
     TYT = std::min(TYT, (g.ny + RY - 1) / RY);
-    const int nthr = ((P2 * TYT + 31) / 32) * 32;
+    {
+        const int nb = (g.ny + TYT * RY - 1) / (TYT * RY);
+        const int ty_bal = (g.ny + nb - 1) / nb;
+        TYT = std::min(TYT, (ty_bal + RY - 1) / RY);
+    }
+    const int nthr = ((P2 * TYT + 31) / 32) * 32 + 32;  // consumer warps + one producer warp
     PipeGeom G;
     G.nx = g.nx;
     G.ny = g.ny;
     G.nz = g.nz;
     G.nxp = nxp;
-    const int q = (int)(16 / sizeof(T)) > 0 ? (int)(16 / sizeof(T)) : 1;
-    const int XOFF = (R % RX == 0) ? R : (R + RX - (R % RX));
-    G.GL = ((XOFF + q - 1) / q) * q;
-    {
-        const int rx_nx = ((g.nx + RX - 1) / RX) * RX;
-        int sp = std::max(G.GL + nxp, G.GL + rx_nx + XOFF + RX);
-        G.SP = ((sp + q - 1) / q) * q;
-    }
+    G.GL = 0;
+    G.SP = nxp;
     G.TYT = TYT;
     G.TY = TYT * RY;
     G.P2 = P2;
@@ -87,11 +101,14 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
     G.zchunk = (g.nz + nzch - 1) / nzch;
     nzch = (g.nz + G.zchunk - 1) / G.zchunk;
     const bool xo = (xold != nullptr) && d != 0.0;
-    const size_t tile_b = (size_t)(G.TY + 2 * R) * G.SP * sizeof(T);
+    const size_t tile_b = (size_t)(G.TY + 2 * R) * nxp * sizeof(T);
     const size_t own_b = (size_t)G.TY * nxp * sizeof(T);
     const size_t v_b = (size_t)G.TY * nxp * sizeof(S);
     const size_t stage = ((tile_b + (xo ? own_b : 0) + v_b + 127) / 128) * 128;
-    const size_t smem = 128 + kPipeStages * stage;
+    // window ring (4 stages of the band's own rows) + as many tile stages (3..5) as fit
+    const size_t wring = 4 * ((own_b + 127) / 128) * 128;
+    int ns = (int)std::min<size_t>(5, (227 * 1024 - 256 - wring) / stage);
+    const size_t smem = 256 + wring + (size_t)std::max(ns, 3) * stage;
     if (smem > 227 * 1024) {
         set_error("pipelined stencil stage of %zu bytes exceeds shared memory", smem);
         return LYNX_ERR_UNSUPPORTED;
@@ -114,11 +131,18 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
         C.phl[k] = phl[k];
         C.phr[k] = phr[k];
     }
+    bool phased = false;
+    for (int k = 0; k < 3; ++k) {
+        const S* l = reinterpret_cast<const S*>(&phl[k]);
+        const S* r = reinterpret_cast<const S*>(&phr[k]);
+        for (int c = 0; c < (int)(sizeof(T) / sizeof(S)); ++c)
+            if (l[c] != (c == 0 ? S(1) : S(0)) || r[c] != (c == 0 ? S(1) : S(0))) phased = true;
+    }
     dim3 grid(nbands, ncol, nzch);
 #define LYNX_PIPE_CASE(RR)                                                                       \
     case RR:                                                                                     \
-        if (xo) launch_pipe<T, RR, true>(grid, nthr, smem, st, x, xold, out, V, G, C, err);       \
-        else launch_pipe<T, RR, false>(grid, nthr, smem, st, x, xold, out, V, G, C, err);         \
+        if (xo) launch_pipe<T, RR, true>(ns, phased, grid, nthr, smem, st, x, xold, out, V, G, C, err);       \
+        else launch_pipe<T, RR, false>(ns, phased, grid, nthr, smem, st, x, xold, out, V, G, C, err);         \
         break;
     switch (R) {
         LYNX_PIPE_CASE(1)
