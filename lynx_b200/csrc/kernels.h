@@ -64,7 +64,7 @@ struct NLDev {
 };
 
 // Column block widths of the nonlocal kernels; alpha rows are padded to a multiple of kNLColBlock.
-constexpr int kNLColBlock = 16;
+constexpr int kNLColBlock = 32;
 
 template <typename T>
 int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alpha, int ncolp, double dV,

@@ -6,7 +6,7 @@
 //   gather : one CTA per (physical atom, block of NB columns) reduces all images
 //            of the atom in a fixed order:
 //              alpha[p][n] = Gamma_p * dV * sum_img e^{-i k.R_img} sum_g chi_img[g,p] psi[gpos[g], n]
-//            The sum runs in FP64 for FP32 data as well.
+//            accumulated in the precision of the data (FP64 or FP32).
 //   scatter: one thread per (distinct grid point in the union of spheres, NB columns)
 //            pulls every (image, local point) entry that lands on its grid point
 //            (CSR built on the host), so no two threads write the same element:
@@ -39,20 +39,6 @@ struct NLView {
     const int* ent_loc;        // sum ndc
 };
 
-template <typename T> struct AccOf;
-template <> struct AccOf<double> { using type = double; };
-template <> struct AccOf<float> { using type = double; };
-template <> struct AccOf<double2> { using type = double2; };
-template <> struct AccOf<float2> { using type = double2; };
-
-__device__ __forceinline__ double to_acc(double v) { return v; }
-__device__ __forceinline__ double to_acc(float v) { return (double)v; }
-__device__ __forceinline__ double2 to_acc(double2 v) { return v; }
-__device__ __forceinline__ double2 to_acc(float2 v) { return make_double2(v.x, v.y); }
-__device__ __forceinline__ void from_acc(double& d, double v) { d = v; }
-__device__ __forceinline__ void from_acc(float& d, double v) { d = (float)v; }
-__device__ __forceinline__ void from_acc(double2& d, double2 v) { d = v; }
-__device__ __forceinline__ void from_acc(float2& d, double2 v) { d = make_float2((float)v.x, (float)v.y); }
 __device__ __forceinline__ double acc_phase(double v, double, double) { return v; }
 __device__ __forceinline__ double2 acc_phase(double2 v, double re, double im) {
     return make_double2(v.x * re - v.y * im, v.x * im + v.y * re);
@@ -60,67 +46,98 @@ __device__ __forceinline__ double2 acc_phase(double2 v, double re, double im) {
 
 constexpr int kGatherTile = 64;  // grid points per shared-memory tile
 
-template <typename T, int NB>
-__global__ void __launch_bounds__(1024)
+// Accumulation type of the gather: FP64 for FP64 data, the data's own precision for FP32
+// data (a sum over one atom's sphere, ~10^3 terms).
+template <typename T> struct GAccOf { using type = T; };
+template <> struct GAccOf<double> { using type = double; };
+__device__ __forceinline__ float2 acc_phase(float2 v, double re, double im) {
+    return make_float2((float)(v.x * re - v.y * im), (float)(v.x * im + v.y * re));
+}
+__device__ __forceinline__ float acc_phase(float v, double, double) { return v; }
+
+// gather: CTA = (atom, NB columns), 256 threads; thread = (column n, projector group jq),
+// projectors jq, jq+8, jq+16, ... (up to PJ of them).  The gathered x tile is staged in
+// shared memory with lanes along the grid points (coalesced loads).
+template <typename T, int NB, int PJ>
+__global__ void __launch_bounds__(256)
     nl_gather_kernel(const T* __restrict__ x, long long ld, int ncol, int ncolp, NLView tab,
                      T* __restrict__ alpha, double dV) {
     using S = typename ScalarOf<T>::type;
-    using Acc = typename AccOf<T>::type;
+    using A = typename GAccOf<T>::type;
     constexpr int G = kGatherTile;
-    constexpr int GP = G + 1;  // padded row: avoids bank conflicts between columns
+    constexpr int NBP = NB + 1;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* sx = reinterpret_cast<T*>(smraw);                       // NB x GP
-    S* schi = reinterpret_cast<S*>(smraw + sizeof(T) * NB * GP);  // np x GP
+    T* xs = reinterpret_cast<T*>(smraw);                          // G x NBP
+    S* cs = reinterpret_cast<S*>(smraw + sizeof(T) * G * NBP);    // G x np
     const S* chi = reinterpret_cast<const S*>(tab.chi);
-
     const int a = blockIdx.x;
     const int n0 = blockIdx.y * NB;
     const int np = tab.atom_nproj[a];
     const int poff = tab.atom_poff[a];
-    const int nout = np * NB;
-    const int tid = threadIdx.x, nthr = blockDim.x;
-    const int jp = tid / NB, nn = tid - (tid / NB) * NB;
-    Acc acc = to_acc(vzero(T()));
+    const int tid = threadIdx.x;
+    const int n = tid % NB;
+    const int jq = tid / NB;
+    constexpr int JG = 256 / NB;  // projector groups
+    A acc[PJ];
+#pragma unroll
+    for (int m = 0; m < PJ; ++m) acc[m] = vzero(A());
     for (int ii = tab.atom_img_ptr[a]; ii < tab.atom_img_ptr[a + 1]; ++ii) {
         const int im = tab.atom_img_list[ii];
         const int ndc = tab.img_ndc[im];
         const int* gp = tab.gpos + tab.img_goff[im];
         const S* ch = chi + tab.img_chi_off[im];
-        Acc part = to_acc(vzero(T()));
+        A part[PJ];
+#pragma unroll
+        for (int m = 0; m < PJ; ++m) part[m] = vzero(A());
         for (int g0 = 0; g0 < ndc; g0 += G) {
             const int gl = min(G, ndc - g0);
             __syncthreads();
-            for (int e = tid; e < G * NB; e += nthr) {
+            for (int e = tid; e < G * NB; e += 256) {
                 const int g = e % G, c = e / G;
                 T v = vzero(T());
                 if (g < gl && n0 + c < ncol) v = x[(long long)gp[g0 + g] + (long long)(n0 + c) * ld];
-                sx[c * GP + g] = v;
+                xs[g * NBP + c] = v;
             }
-            for (int e = tid; e < G * np; e += nthr) {
+            for (int e = tid; e < G * np; e += 256) {
                 const int g = e % G, j = e / G;
-                schi[j * GP + g] = (g < gl) ? ch[(long long)j * ndc + g0 + g] : S(0);
+                cs[g * np + j] = (g < gl) ? ch[(long long)j * ndc + g0 + g] : S(0);
             }
             __syncthreads();
-            if (tid < nout) {
-                const S* cr = schi + jp * GP;
-                const T* xr = sx + nn * GP;
-                for (int g = 0; g < gl; ++g) part = fmac(part, (double)cr[g], to_acc(xr[g]));
+            for (int g = 0; g < gl; ++g) {
+                const T xv = xs[g * NBP + n];
+#pragma unroll
+                for (int m = 0; m < PJ; ++m) {
+                    const int j = jq + m * JG;
+                    if (j < np) part[m] = fmac(part[m], (S)cs[g * np + j], xv);
+                }
             }
         }
-        acc = vadd(acc, acc_phase(part, tab.img_phase[2 * im], tab.img_phase[2 * im + 1]));
+#pragma unroll
+        for (int m = 0; m < PJ; ++m)
+            acc[m] = vadd(acc[m], acc_phase(part[m], tab.img_phase[2 * im], tab.img_phase[2 * im + 1]));
     }
-    if (tid < nout) {
-        T out;
-        from_acc(out, vscale(tab.gamma[poff + jp] * dV, acc));
-        alpha[(long long)(poff + jp) * ncolp + n0 + nn] = out;
+#pragma unroll
+    for (int m = 0; m < PJ; ++m) {
+        const int j = jq + m * JG;
+        if (j < np) alpha[(long long)(poff + j) * ncolp + n0 + n] = vscale((S)(tab.gamma[poff + j] * dV), acc[m]);
     }
 }
 
+template <typename T, int V> struct VecN;
+template <> struct VecN<float, 4> { using type = float4; };
+template <> struct VecN<double, 2> { using type = double2; };
+template <> struct VecN<float2, 2> { using type = float4; };
+template <> struct VecN<double2, 1> { using type = double2; };
+
+// scatter: one thread per (distinct grid point, NB columns); alpha rows read as vectors.
 template <typename T, int NB>
 __global__ void __launch_bounds__(128)
     nl_scatter_kernel(T* __restrict__ out, long long ld, int ncol, int ncolp, NLView tab,
                       const T* __restrict__ alpha, typename ScalarOf<T>::type scale) {
     using S = typename ScalarOf<T>::type;
+    constexpr int VW = 16 / sizeof(T);  // elements per 16-byte vector
+    using VV = typename VecN<T, VW>::type;
+    static_assert(NB % VW == 0, "column block must be a multiple of the vector width");
     const S* chi = reinterpret_cast<const S*>(tab.chi);
     const int u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= tab.n_pts) return;
@@ -141,9 +158,14 @@ __global__ void __launch_bounds__(128)
         for (int k = 0; k < NB; ++k) tmp[k] = vzero(T());
         for (int j = 0; j < np; ++j) {
             const S c = ch[(long long)j * ndc];
-            const T* al = alpha + (long long)(poff + j) * ncolp + n0;
+            const VV* al = reinterpret_cast<const VV*>(alpha + (long long)(poff + j) * ncolp + n0);
 #pragma unroll
-            for (int k = 0; k < NB; ++k) tmp[k] = fmac(tmp[k], c, al[k]);
+            for (int q = 0; q < NB / VW; ++q) {
+                const VV v = __ldg(al + q);
+                const T* ve = reinterpret_cast<const T*>(&v);
+#pragma unroll
+                for (int k = 0; k < VW; ++k) tmp[q * VW + k] = fmac(tmp[q * VW + k], c, ve[k]);
+            }
         }
         if constexpr (ScalarOf<T>::cplx) {
             // conj of the gather phase: e^{+i k.R_img}

@@ -37,18 +37,24 @@ template <typename T>
 int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alpha, int ncolp, double dV,
                      cudaStream_t st) {
     using S = typename ScalarOf<T>::type;
-    constexpr int NB = kNLColBlock;
+    constexpr int NB = 32;  // columns per CTA; 8 projector groups of 256 threads
+    static_assert(kNLColBlock % 16 == 0 && NB % kNLColBlock == 0 || kNLColBlock % NB == 0, "column blocks");
     if (nl.n_atom == 0 || ncol <= 0) return LYNX_OK;
-    const int nthr = ((nl.max_np * NB + 31) / 32) * 32;
-    if (nthr > 1024) {
-        set_error("%d projectors per atom exceed the gather kernel's block", nl.max_np);
+    const int pj = (nl.max_np + 7) / 8;
+    if (pj > 4) {
+        set_error("%d projectors per atom exceed the gather kernel's limit of 32", nl.max_np);
         return LYNX_ERR_UNSUPPORTED;
     }
-    const size_t smem = sizeof(T) * NB * (kGatherTile + 1) + sizeof(S) * nl.max_np * (kGatherTile + 1);
-    auto kern = nl_gather_kernel<T, NB>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const size_t smem = sizeof(T) * kGatherTile * (NB + 1) + sizeof(S) * nl.max_np * kGatherTile;
     dim3 grid(nl.n_atom, (ncol + NB - 1) / NB);
-    kern<<<grid, nthr, smem, st>>>(x, ld, ncol, ncolp, make_view<T>(nl), alpha, dV);
+    auto go = [&](auto kern) {
+        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 256, smem, st>>>(x, ld, ncol, ncolp, make_view<T>(nl), alpha, dV);
+    };
+    if (pj <= 1) go(nl_gather_kernel<T, NB, 1>);
+    else if (pj == 2) go(nl_gather_kernel<T, NB, 2>);
+    else if (pj == 3) go(nl_gather_kernel<T, NB, 3>);
+    else go(nl_gather_kernel<T, NB, 4>);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -61,7 +67,7 @@ int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alp
 template <typename T, typename S>
 int launch_nl_scatter(const NLDev& nl, T* out, long long ld, int ncol, const T* alpha, int ncolp, S scale,
                       cudaStream_t st) {
-    constexpr int NB = 8;
+    constexpr int NB = 16;
     if (nl.n_pts == 0 || ncol <= 0) return LYNX_OK;
     dim3 grid((nl.n_pts + 127) / 128, (ncol + NB - 1) / NB);
     nl_scatter_kernel<T, NB><<<grid, 128, 0, st>>>(out, ld, ncol, ncolp, make_view<T>(nl), alpha, scale);
