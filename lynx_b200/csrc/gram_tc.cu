@@ -1,0 +1,429 @@
+// Rayleigh-Ritz Gram products on the 5th-generation tensor cores (sm_100a):
+//   Ms = dV * Y^T Y,   Hs = dV * Y^T (HY)                  (N x N, FP64 result)
+// for FP32 blocks Y, HY of K = Nd grid points x N states (src/solvers/EigenSolver.cpp:622-660,
+// the overlap and projected-Hamiltonian products of the Rayleigh-Ritz step).
+//
+// Precision (integer split, "Ozaki" scheme): the K range is cut into split chunks; in each
+// chunk every state column j is scaled by a power of two 2^-e_j (|y| 2^-e < 1/2) and written
+// as three signed 7-bit slices,
+//     y = 2^e (s1 2^-7 + s2 2^-14 + s3 2^-21) + r,   s_a in [-64, 64],  |r| <= 2^(e-22),
+// each slice rounded to nearest (unbiased).  The slice products with a+b <= 4 are formed by
+// tcgen05.mma kind::i8 into three int32 accumulators in tensor memory (one per weight
+// 2^-14, 2^-21, 2^-28), which is exact: no rounding at all happens in the tensor cores.
+// The epilogue combines the three levels exactly in FP64 and applies 2^(e_i+e_j); the split
+// partials are summed in FP64.  The only approximation is the slice representation
+// (relative 2^-20 of the column's largest element, unbiased), far below the FP32 rounding
+// of Y itself once summed over K.  (FP32-accumulating bf16 products were measured on this
+// hardware to carry an accumulation bias that grows with K, ~1e-4 relative at 7e5 points.)
+//
+// Kernel structure (one CTA = one 128 x 128 output tile x one K chunk, 4 warps):
+//   warp 0 lane 0  : TMA producer, 2-stage ring of the 6 slice tiles (A s1..s3, B s1..s3),
+//                    128 rows x 128 int8 each, in the 128-byte-swizzled K-major layout;
+//   warp 1 lane 0  : MMA issuer, 24 MMAs per stage (4 K32 sub-steps x 6 slice products),
+//                    then tcgen05.commit to release the stage;
+//   all 4 warps    : epilogue, tcgen05.ld of the three 128 x 128 int32 accumulators (warp w
+//                    owns TMEM lanes 32w..32w+31) and a store of the FP64 partial tile.
+// Ms needs only its upper triangle (the Cholesky reads it), so only tiles tm <= tn run.
+// Every mbarrier wait is bounded; a timeout sets the error flag, and tensor memory is
+// always released before the CTA exits.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cstdint>
+#include <cstring>
+
+#include "kernels.h"
+#include "lynx_common.cuh"
+#include "stencil_pipe.cuh"
+
+namespace lynxb {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 128, STAGES = 2;  // BK: int8 K elements (= bytes) per stage row
+constexpr int NSLICE = 3;
+constexpr int TILE_BYTES = BM * BK;                      // 16 KB, one slice tile
+constexpr int STAGE_BYTES = 2 * NSLICE * TILE_BYTES;     // A and B slices: 96 KB
+constexpr int TMEM_COLS = 512;                           // 3 accumulators x 128 columns, power of two
+constexpr int kMaxChunkSteps = 1365;  // 3 * 64 * 64 * 128 * 1365 < 2^31: int32 accumulators cannot overflow
+// kind::i8 instruction descriptor: D = S32 (bits 4-5 = 2), A = B = signed 8-bit (bits 7-9,
+// 10-12 = 1), K-major A and B, N>>3 at bits 17-22, M>>4 at bits 24-28.
+constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+// Shared-memory matrix descriptor for a K-major tile of 128-byte rows, 128-byte swizzle:
+// 8-row core groups 1024 bytes apart (stride byte offset), descriptor version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1u << 16;              // leading byte offset (unused by swizzled K-major)
+    d |= (uint64_t)(1024u >> 4) << 32;    // stride byte offset
+    d |= (uint64_t)1u << 46;              // version
+    d |= (uint64_t)2u << 61;              // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(IDESC), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+struct GramArgs {
+    int ksteps;     // K steps of BK over the whole (padded) K range
+    int kper;       // K steps per split
+    int nsplit;
+    int T;          // tiles along N
+    int ntri;       // T (T + 1) / 2: upper-triangular tile pairs of Ms
+    int npad;       // T * 128
+    const int* eY;  // [nsplit][npad] column exponents of Y
+    const int* eH;  // [nsplit][npad] column exponents of HY
+    double* ws;     // [2][nsplit][npad][npad] FP64 partial tiles
+    int* err;
+};
+
+__global__ void __launch_bounds__(128, 1)
+    gram_i8_kernel(const __grid_constant__ CUtensorMap tY1, const __grid_constant__ CUtensorMap tY2,
+                   const __grid_constant__ CUtensorMap tY3, const __grid_constant__ CUtensorMap tH1,
+                   const __grid_constant__ CUtensorMap tH2, const __grid_constant__ CUtensorMap tH3,
+                   const GramArgs g) {
+    extern __shared__ __align__(1024) unsigned char gsm[];
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(gsm) + 1023) & ~static_cast<uintptr_t>(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* done = empty + STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int prod, tm, tn;
+    if ((int)blockIdx.x < g.ntri) {  // Ms: tile pairs tm <= tn, row by row
+        prod = 0;
+        int r = blockIdx.x;
+        tm = 0;
+        while (r >= g.T - tm) {
+            r -= g.T - tm;
+            ++tm;
+        }
+        tn = tm + r;
+    } else {
+        prod = 1;
+        const int r = blockIdx.x - g.ntri;
+        tm = r / g.T;
+        tn = r % g.T;
+    }
+    const int m0 = tm * BM, n0 = tn * BN;
+    const int split = blockIdx.y;
+    const int k0 = split * g.kper;
+    const int nk = min(g.ksteps, k0 + g.kper) - k0;
+    const CUtensorMap* mA[NSLICE] = {&tY1, &tY2, &tY3};
+    const CUtensorMap* mB[NSLICE] = {prod ? &tH1 : &tY1, prod ? &tH2 : &tY2, prod ? &tH3 : &tY3};
+    auto tileA = [&](int s, int q) { return base + s * STAGE_BYTES + q * TILE_BYTES; };
+    auto tileB = [&](int s, int q) { return base + s * STAGE_BYTES + (NSLICE + q) * TILE_BYTES; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    const int row = m0 + warp * 32 + lane;
+    double* wrow = g.ws + (((long long)prod * g.nsplit + split) * g.npad + row) * g.npad + n0;
+    bool ok = true;
+    if (nk > 0) {
+        if (warp == 0 && lane == 0) {
+            for (int k = 0; k < nk; ++k) {
+                const int s = k % STAGES, u = k / STAGES;
+                if (u > 0 && !mbar_wait(&empty[s], (uint32_t)((u - 1) & 1))) {
+                    ok = false;
+                    break;
+                }
+                mbar_expect_tx(&full[s], STAGE_BYTES);
+                const int x = (k0 + k) * BK;
+#pragma unroll
+                for (int q = 0; q < NSLICE; ++q) {
+                    tma_load_2d(tileA(s, q), mA[q], x, m0, &full[s]);
+                    tma_load_2d(tileB(s, q), mB[q], x, n0, &full[s]);
+                }
+            }
+        } else if (warp == 1 && lane == 0) {
+            for (int k = 0; k < nk; ++k) {
+                const int s = k % STAGES, u = k / STAGES;
+                if (!mbar_wait(&full[s], (uint32_t)(u & 1))) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                uint64_t a[NSLICE], b[NSLICE];
+#pragma unroll
+                for (int q = 0; q < NSLICE; ++q) {
+                    a[q] = sw128_desc(smem_u32(tileA(s, q)));
+                    b[q] = sw128_desc(smem_u32(tileB(s, q)));
+                }
+#pragma unroll
+                for (int kk = 0; kk < BK / 32; ++kk) {
+                    const uint64_t off = (uint64_t)(kk * 32) >> 4;  // K32 sub-step = 32 bytes along the row
+                    const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+                    mma_i8(tmem + 0, a[0] + off, b[0] + off, acc);        // weight 2^-14
+                    mma_i8(tmem + 128, a[0] + off, b[1] + off, acc);      // weight 2^-21
+                    mma_i8(tmem + 128, a[1] + off, b[0] + off, 1u);
+                    mma_i8(tmem + 256, a[0] + off, b[2] + off, acc);      // weight 2^-28
+                    mma_i8(tmem + 256, a[1] + off, b[1] + off, 1u);
+                    mma_i8(tmem + 256, a[2] + off, b[0] + off, 1u);
+                }
+                mma_commit(&empty[s]);
+            }
+            mma_commit(done);
+        }
+        __syncwarp();
+        if (!mbar_wait(done, 0)) ok = false;
+        // tcgen05.ld is warp-collective (.sync.aligned): the decision must be warp-uniform
+        ok = __all_sync(0xffffffffu, ok);
+        tc_fence_after();
+        if (ok) {
+            const int* eA = g.eY + (long long)split * g.npad;
+            const int* eB = (prod ? g.eH : g.eY) + (long long)split * g.npad;
+            const int ea = eA[row];
+            const uint32_t lb = (uint32_t)(warp * 32) << 16;
+#pragma unroll 1
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                uint32_t r2[16], r3[16], r4[16];
+                tmem_ld16(tmem + lb + (uint32_t)c0, r2);
+                tmem_ld16(tmem + lb + 128u + (uint32_t)c0, r3);
+                tmem_ld16(tmem + lb + 256u + (uint32_t)c0, r4);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                double v[16];
+#pragma unroll
+                for (int t = 0; t < 16; ++t) {
+                    // exact: the three terms span bits 2^17 .. 2^-28 (< 53 bits)
+                    const double x = (double)(int)r2[t] * 0x1p-14 + (double)(int)r3[t] * 0x1p-21 +
+                                     (double)(int)r4[t] * 0x1p-28;
+                    v[t] = ldexp(x, ea + eB[n0 + c0 + t]);
+                }
+                double2* dst = reinterpret_cast<double2*>(wrow + c0);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) dst[q] = make_double2(v[2 * q], v[2 * q + 1]);
+            }
+        }
+    } else {
+        for (int c = 0; c < BN; ++c) wrow[c] = 0.0;  // empty K chunk: the partial tile is zero
+    }
+    if (!ok && lane == 0) atomicExch(g.err, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// One K chunk of one column of an FP32 block -> exponent e and three int8 slices (column
+// stride ldk; rows rows..ldk-1 of the padded K range written as zero).
+__global__ void __launch_bounds__(256)
+    slice_i8_kernel(int8_t* __restrict__ s1, int8_t* __restrict__ s2, int8_t* __restrict__ s3, long long ldk,
+                    int* __restrict__ eexp, int npad, const float* __restrict__ y, long long ldy, long long rows,
+                    long long chunk) {
+    __shared__ float red[8];
+    const int split = blockIdx.x, j = blockIdx.y;
+    const long long r0 = (long long)split * chunk;
+    const long long r1 = min(r0 + chunk, ldk);
+    const long long rend = min(r1, rows);
+    const float* col = y + (long long)j * ldy;
+    float m = 0.0f;
+    for (long long r = r0 + threadIdx.x; r < rend; r += blockDim.x) m = fmaxf(m, fabsf(col[r]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = red[0];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) m = fmaxf(m, red[w]);
+    int E = 0;
+    if (m > 0.0f) frexpf(m, &E);  // m = f 2^E, f in [1/2, 1)
+    const int e = (m > 0.0f) ? E + 1 : 0;  // |y| 2^-e < 1/2
+    if (threadIdx.x == 0) eexp[(long long)split * npad + j] = e;
+    int8_t* o1 = s1 + (long long)j * ldk;
+    int8_t* o2 = s2 + (long long)j * ldk;
+    int8_t* o3 = s3 + (long long)j * ldk;
+    for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+        float t = (r < rows) ? ldexpf(col[r], 7 - e) : 0.0f;  // exact: power-of-two scaling
+        const float a = rintf(t);                               // |t| < 64
+        t = (t - a) * 128.0f;                                   // exact, |t| <= 64
+        const float b = rintf(t);
+        t = (t - b) * 128.0f;
+        const float c = rintf(t);
+        o1[r] = (int8_t)(int)a;
+        o2[r] = (int8_t)(int)b;
+        o3[r] = (int8_t)(int)c;
+    }
+}
+
+// Ms / Hs (column-major N x N, FP64) = dV * sum over splits of the FP64 partial tiles;
+// Ms only for tiles on or above the diagonal.
+__global__ void gram_reduce_kernel(double* __restrict__ Ms, double* __restrict__ Hs, const double* __restrict__ ws,
+                                   int nsplit, int npad, int n, double dV) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // column
+    const int i = blockIdx.y;                             // row
+    const int prod = blockIdx.z;
+    if (j >= n) return;
+    if (prod == 0 && (i / BM) > (j / BN)) return;
+    double s = 0.0;
+    const double* p = ws + ((long long)prod * nsplit * npad + i) * npad + j;
+    for (int t = 0; t < nsplit; ++t) s += p[(long long)t * npad * npad];
+    (prod ? Hs : Ms)[i + (long long)j * n] = dV * s;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 2-D int8 tensor [rows][ldk] (ldk contiguous), box 128 x 128, 128-byte swizzle.
+int make_map(CUtensorMap* m, const int8_t* ptr, long long ldk, int rows) {
+    auto enc = get_encode();
+    if (!enc) {
+        set_error("cuTensorMapEncodeTiled is not available");
+        return LYNX_ERR_CUDA;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)ldk, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ldk};
+    cuuint32_t box[2] = {BK, BM};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(ptr), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+}  // namespace
+
+GramPlan gram_plan(long long rows, int n) {
+    GramPlan p;
+    p.ldk = ((rows + BK - 1) / BK) * BK;
+    const int ksteps = (int)(p.ldk / BK);
+    const int T = (n + BM - 1) / BM;
+    p.npad = T * BM;
+    const int tiles = T * (T + 1) / 2 + T * T;
+    const int need = (ksteps + kMaxChunkSteps - 1) / kMaxChunkSteps;
+    int ns = std::max(1, (4 * 148) / tiles);  // about four waves of CTAs over 148 SMs
+    ns = std::max(ns, need);
+    ns = std::min(ns, ksteps);
+    const int kper = (ksteps + ns - 1) / ns;
+    p.nsplit = (ksteps + kper - 1) / kper;  // no empty chunks
+    p.kper = kper;
+    p.slice_bytes = align256((size_t)p.ldk * n);
+    p.exp_bytes = align256((size_t)p.nsplit * p.npad * sizeof(int));
+    p.ws_bytes = (size_t)2 * p.nsplit * p.npad * p.npad * sizeof(double);
+    p.work_bytes = 6 * p.slice_bytes + 2 * p.exp_bytes + p.ws_bytes;
+    return p;
+}
+
+int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows, int n, double dV,
+                   const GramPlan& p, void* work, size_t work_bytes, double* Ms, double* Hs, int* err,
+                   cudaStream_t st) {
+    if (work_bytes < p.work_bytes || (reinterpret_cast<uintptr_t>(work) & 255)) {
+        set_error("Gram workspace too small or misaligned");
+        return LYNX_ERR_BAD_ARG;
+    }
+    unsigned char* w = static_cast<unsigned char*>(work);
+    int8_t* sl[6];
+    for (int q = 0; q < 6; ++q) sl[q] = reinterpret_cast<int8_t*>(w + q * p.slice_bytes);
+    int* eY = reinterpret_cast<int*>(w + 6 * p.slice_bytes);
+    int* eH = reinterpret_cast<int*>(w + 6 * p.slice_bytes + p.exp_bytes);
+    double* ws = reinterpret_cast<double*>(w + 6 * p.slice_bytes + 2 * p.exp_bytes);
+    const long long chunk = (long long)p.kper * BK;
+    {
+        dim3 grid(p.nsplit, n);
+        slice_i8_kernel<<<grid, 256, 0, st>>>(sl[0], sl[1], sl[2], p.ldk, eY, p.npad, Y, ld, rows, chunk);
+        slice_i8_kernel<<<grid, 256, 0, st>>>(sl[3], sl[4], sl[5], p.ldk, eH, p.npad, HY, ld, rows, chunk);
+        count_launch(2);
+    }
+    CUtensorMap m[6];
+    for (int q = 0; q < 6; ++q) LYNX_TRY(make_map(&m[q], sl[q], p.ldk, n));
+    GramArgs g;
+    g.ksteps = (int)(p.ldk / BK);
+    g.kper = p.kper;
+    g.nsplit = p.nsplit;
+    g.T = p.npad / BM;
+    g.ntri = g.T * (g.T + 1) / 2;
+    g.npad = p.npad;
+    g.eY = eY;
+    g.eH = eH;
+    g.ws = ws;
+    g.err = err;
+    const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
+    LYNX_CUDA_TRY(cudaFuncSetAttribute(gram_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(g.ntri + g.T * g.T, p.nsplit);
+    gram_i8_kernel<<<grid, 128, smem, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], g);
+    {
+        dim3 rg((n + 127) / 128, n, 2);
+        gram_reduce_kernel<<<rg, 128, 0, st>>>(Ms, Hs, ws, p.nsplit, p.npad, n, dV);
+    }
+    count_launch(2);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("Gram kernel launch failed: %s", cudaGetErrorString(e));
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+}  // namespace lynxb

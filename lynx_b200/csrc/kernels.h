@@ -34,6 +34,20 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
                      long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl, const T* phr,
                      int* err, cudaStream_t st);
 
+// Rayleigh-Ritz Gram products Ms = dV Y^T Y (upper triangle), Hs = dV Y^T HY of FP32 blocks
+// (rows x n, column stride ld) on the tensor cores: exact int8-slice products, FP64 result,
+// Ms/Hs n x n column-major.  work: gram_plan(rows, n).work_bytes, 256-byte aligned.
+struct GramPlan {
+    long long ldk;      // padded K (rows) of the slice arrays
+    int npad;           // N rounded up to the 128-state tile
+    int nsplit, kper;   // K chunks and 128-row K steps per chunk
+    size_t slice_bytes, exp_bytes, ws_bytes, work_bytes;
+};
+GramPlan gram_plan(long long rows, int n);
+int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows, int n, double dV,
+                   const GramPlan& p, void* work, size_t work_bytes, double* Ms, double* Hs, int* err,
+                   cudaStream_t st);
+
 // Launches issued by the library (diagnostic counter, incremented by every launcher).
 void count_launch(int n = 1);
 

@@ -49,6 +49,7 @@ void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    int tag = 0;  // layout the contents were written in (0 = none)
     int ensure(size_t b) {
         if (b <= bytes) return LYNX_OK;
         if (p) cudaFree(p);
@@ -165,6 +166,8 @@ struct lynx_ctx {
     DevBuf io_psi, io_v;  // staging for the host-pointer solve
     DevBuf vpad64, vpad32;  // Veff in the padded row layouts of the pipelined stencil
     DevBuf errflag;         // set by a kernel whose bounded wait gave up
+    DevBuf gwork;           // slices, exponents and split partials of the tensor-core Gram
+    bool no_tc_gram = false;  // diagnostic switch: FP64 library products for the mixed path
     // nonlocal tables re-indexed for padded row layouts: nxp -> tables
     std::map<int, NLDev> nl_layouts;
     std::vector<DevBuf> nl_layout_bufs;
@@ -376,6 +379,20 @@ int ensure_zeroed(lynx_ctx* c, DevBuf& b, size_t bytes) {
     return LYNX_OK;
 }
 
+// Work buffer in a given row layout (tag): grown and/or re-zeroed when the layout changes,
+// so padding elements never hold bytes of another layout.
+int ensure_layout(lynx_ctx* c, DevBuf& b, size_t bytes, int tag) {
+    if (bytes > b.bytes) {
+        LYNX_TRY(b.ensure(bytes));
+        b.tag = -1;
+    }
+    if (b.tag != tag) {
+        LYNX_CUDA_TRY(cudaMemsetAsync(b.p, 0, b.bytes, c->stream));
+        b.tag = tag;
+    }
+    return LYNX_OK;
+}
+
 // Copy/convert the valid points of ncol columns between row layouts (row length nxp, column stride ld).
 template <typename Dst, typename Src>
 __global__ void repack_kernel(Dst* __restrict__ dst, int dnxp, long long dld, const Src* __restrict__ src, int snxp,
@@ -547,7 +564,8 @@ int run_filter64(lynx_ctx* c, const T64* X, long long ldX, const double* veff, i
     *ldb = (long long)(*nxp) * c->ny * c->nz;
     const size_t blk = sizeof(T64) * (size_t)(*ldb) * N;
     const bool direct = (*nxp == c->nx) && (ldX * sizeof(T64)) % 16 == 0 && aligned16(X);
-    for (int i = 0; i < (direct ? 3 : 4); ++i) LYNX_TRY(ensure_zeroed(c, c->wbuf[i], blk));
+    const int tag = (int)(sizeof(T64) * 1000 + *nxp);
+    for (int i = 0; i < (direct ? 3 : 4); ++i) LYNX_TRY(ensure_layout(c, c->wbuf[i], blk, tag));
     const S* Vp = nullptr;
     LYNX_TRY(veff_layout<S>(c, veff, *nxp, &Vp));
     const T64* Xin = X;
@@ -574,7 +592,8 @@ int run_filter32(lynx_ctx* c, const T64* X, long long ldX, const double* veff, i
     *nxp = pipe_capable<T32>(c->nx) ? pipe_row_elems(c->nx, sizeof(S)) : c->nx;
     *ldb = (long long)(*nxp) * c->ny * c->nz;
     const size_t blk = sizeof(T32) * (size_t)(*ldb) * N;
-    for (int i = 0; i < 4; ++i) LYNX_TRY(ensure_zeroed(c, c->wbuf[i], blk));
+    const int tag = (int)(sizeof(T32) * 1000 + *nxp);
+    for (int i = 0; i < 4; ++i) LYNX_TRY(ensure_layout(c, c->wbuf[i], blk, tag));
     const S* Vp = nullptr;
     LYNX_TRY(veff_layout<S>(c, veff, *nxp, &Vp));
     T32* X32 = c->wbuf[3].as<T32>();
@@ -632,21 +651,14 @@ int finish_rr(lynx_ctx* c, int N, double* eig_host) {
     return LYNX_OK;
 }
 
-// psi_out = Y R^-1 Q, eig = eig(R^-T (dV Y^T HY) R^-1), R^T R = dV Y^T Y.
-int rayleigh_ritz_real(lynx_ctx* c, const double* Y, long long ldY, const double* HY, long long ldH,
-                       double* psi, long long ldp, int N, double* eig_host) {
-    const size_t nn = (size_t)N * N;
-    LYNX_TRY(c->Ms.ensure(nn * sizeof(double)));
-    LYNX_TRY(c->Hs.ensure(nn * sizeof(double)));
-    LYNX_TRY(c->eigd.ensure(N * sizeof(double)));
-    LYNX_TRY(c->info.ensure(2 * sizeof(int)));
+// Subspace part of the Rayleigh-Ritz step, given Ms = dV Y^T Y and Hs = dV Y^T HY in c->Ms /
+// c->Hs (Ms: at least the upper triangle): Hs' = R^-T sym(Hs) R^-1 with R^T R = Ms,
+// eigenpairs of Hs', W = R^-1 Q, psi = Yrot W.  Yrot: FP64 block with Nd rows.
+int rr_subspace_real(lynx_ctx* c, const double* Yrot, long long ldY, double* psi, long long ldp, int N,
+                     double* eig_host) {
     double* Ms = c->Ms.as<double>();
     double* Hs = c->Hs.as<double>();
-    const double dV = c->dV, one = 1.0, zero = 0.0;
-    CUBLAS_TRY(cublasSetStream(c->cublas, c->stream));
-    CUSOLVER_TRY(cusolverDnSetStream(c->cusolver, c->stream));
-    CUBLAS_TRY(cublasDsyrk(c->cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, N, c->Nd, &dV, Y, ldY, &zero, Ms, N));
-    CUBLAS_TRY(cublasDgemm(c->cublas, CUBLAS_OP_T, CUBLAS_OP_N, N, N, c->Nd, &dV, Y, ldY, HY, ldH, &zero, Hs, N));
+    const double one = 1.0, zero = 0.0;
     {
         dim3 b(16, 16), g((N + 15) / 16, (N + 15) / 16);
         symmetrize_kernel<<<g, b, 0, c->stream>>>(Hs, N);
@@ -670,8 +682,47 @@ int rayleigh_ritz_real(lynx_ctx* c, const double* Y, long long ldY, const double
                                   c->eigd.as<double>(), c->solver_work.as<double>(), lw, info + 1));
     CUBLAS_TRY(cublasDtrsm(c->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
                            N, N, &one, Ms, N, Hs, N));
-    CUBLAS_TRY(cublasDgemm(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, c->Nd, N, N, &one, Y, ldY, Hs, N, &zero, psi, ldp));
+    CUBLAS_TRY(cublasDgemm(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, c->Nd, N, N, &one, Yrot, ldY, Hs, N, &zero, psi, ldp));
     return finish_rr(c, N, eig_host);
+}
+
+int rr_alloc_small(lynx_ctx* c, int N, size_t elem) {
+    const size_t nn = (size_t)N * N;
+    LYNX_TRY(c->Ms.ensure(nn * elem));
+    LYNX_TRY(c->Hs.ensure(nn * elem));
+    LYNX_TRY(c->eigd.ensure(N * sizeof(double)));
+    LYNX_TRY(c->info.ensure(2 * sizeof(int)));
+    CUBLAS_TRY(cublasSetStream(c->cublas, c->stream));
+    CUSOLVER_TRY(cusolverDnSetStream(c->cusolver, c->stream));
+    return LYNX_OK;
+}
+
+// psi_out = Y R^-1 Q, eig = eig(R^-T (dV Y^T HY) R^-1), R^T R = dV Y^T Y; products by cuBLAS (FP64).
+int rayleigh_ritz_real(lynx_ctx* c, const double* Y, long long ldY, const double* HY, long long ldH,
+                       double* psi, long long ldp, int N, double* eig_host) {
+    LYNX_TRY(rr_alloc_small(c, N, sizeof(double)));
+    const double dV = c->dV, zero = 0.0;
+    CUBLAS_TRY(cublasDsyrk(c->cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, N, c->Nd, &dV, Y, ldY, &zero,
+                           c->Ms.as<double>(), N));
+    CUBLAS_TRY(cublasDgemm(c->cublas, CUBLAS_OP_T, CUBLAS_OP_N, N, N, c->Nd, &dV, Y, ldY, HY, ldH, &zero,
+                           c->Hs.as<double>(), N));
+    return rr_subspace_real(c, Y, ldY, psi, ldp, N, eig_host);
+}
+
+// Mixed precision, real: Gram products of the FP32 blocks on the tensor cores (exact int8
+// slice products, FP64 combination), subspace algebra in FP64, rotation of an FP64 copy of Y.
+int rayleigh_ritz_mixed_real(lynx_ctx* c, const float* Y32, const float* HY32, long long ldb, int nxp, double* psi,
+                             long long ldp, int N, double* eig_host) {
+    LYNX_TRY(rr_alloc_small(c, N, sizeof(double)));
+    const GramPlan plan = gram_plan(ldb, N);  // all ldb rows: pad elements are zero
+    LYNX_TRY(c->gwork.ensure(plan.work_bytes));
+    if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
+    LYNX_TRY(launch_gram_i8(Y32, HY32, ldb, ldb, N, c->dV, plan, c->gwork.p, c->gwork.bytes, c->Ms.as<double>(),
+                            c->Hs.as<double>(), c->errflag.as<int>(), c->stream));
+    const long long Nd = c->Nd;
+    LYNX_TRY(c->cvt[0].ensure(sizeof(double) * (size_t)Nd * N));
+    LYNX_TRY(repack<double, float>(c, c->cvt[0].as<double>(), c->nx, Nd, Y32, nxp, ldb, N));
+    return rr_subspace_real(c, c->cvt[0].as<double>(), Nd, psi, ldp, N, eig_host);
 }
 
 int rayleigh_ritz_cplx(lynx_ctx* c, const double2* Y, long long ldY, const double2* HY, long long ldH,
@@ -768,6 +819,14 @@ int solve_impl(lynx_ctx* c, T64* psi, double* eig, const double* veff, int N, in
         T32 *Y = nullptr, *HY = nullptr;
         LYNX_TRY(run_filter32<T32, T64>(c, psi, ldp, veff, N, lc, emin, emax, degree, use_k, true, &Y, &HY, &ldb,
                                         &nxp));
+        if constexpr (std::is_same<T32, float>::value) {
+            if (pipe_capable<float>(c->nx) && !c->no_tc_gram) {
+                LYNX_TRY(rayleigh_ritz_mixed_real(c, Y, HY, ldb, nxp, reinterpret_cast<double*>(psi), ldp, N, eig));
+                LYNX_TRY(check_errflag(c));
+                if (lc_out) *lc_out = eig[N - 1] + 0.1;
+                return LYNX_OK;
+            }
+        }
         // Rayleigh-Ritz products on FP64 copies of the FP32 blocks.
         LYNX_TRY(c->cvt[0].ensure(blk64));
         LYNX_TRY(c->cvt[1].ensure(blk64));
@@ -1072,6 +1131,7 @@ int lynx_destroy(lynx_ctx* c) {
     c->vpad64.release();
     c->vpad32.release();
     c->errflag.release();
+    c->gwork.release();
     for (auto& b : c->nl_layout_bufs) b.release();
     if (c->cublas) cublasDestroy(c->cublas);
     if (c->cusolver) cusolverDnDestroy(c->cusolver);
@@ -1399,7 +1459,7 @@ int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precisi
     const size_t esz = precision == LYNX_PREC_FP64 ? sizeof(double) : sizeof(float);
     const int nxp = (c->nx % 2 == 0) ? pipe_row_elems(c->nx, esz) : c->nx;
     const long long ldb = (long long)nxp * c->ny * c->nz;
-    for (int i = 0; i < 3; ++i) LYNX_TRY(ensure_zeroed(c, c->wbuf[i], esz * (size_t)ldb * ncol));
+    for (int i = 0; i < 3; ++i) LYNX_TRY(ensure_layout(c, c->wbuf[i], esz * (size_t)ldb * ncol, (int)(esz * 1000 + nxp)));
     const bool nl = c->has_nl;
     if (!with_nonlocal) c->has_nl = false;
     cudaEvent_t e0, e1;

@@ -223,3 +223,23 @@ def test_free_particle_known_answer(n):
     V = 0.3 + 0.1 * np.cos(np.tile(x, n * n))
     y2 = H.apply(np.ones(ctx.nd), V)
     assert np.abs(y2 - V).max() < 1e-10
+
+
+@pytest.mark.parametrize("nstates", [150])
+def test_mixed_pass_tensor_core_gram(system, nstates):
+    """Mixed precision real pass (FP32 filter, BF16x3 tensor-core Gram products with FP64
+    split-K reduction, FP64 subspace algebra) against the FP64 pass from the same start:
+    more than one 128-state output tile, a ragged last tile.  Ritz values agree to 2e-5 Ha
+    (FP32 filter rounding dominates), the spectrum stays ordered and both passes span the
+    same subspace."""
+    s = system
+    lo, hi, lc = _bounds(s)
+    psi0 = C.random_orbitals(s["ctx"].nd, nstates, seed=151)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        es = s["solver"].EigenSolver(s["ctx"], prec)
+        out[prec] = es.solve(psi0, s["V"], lc, lo, hi, 10)
+    eig64, eigm = out["fp64"][1], out["mixed"][1]
+    assert np.all(np.diff(eigm) >= -1e-9)
+    assert np.abs(eigm - eig64).max() < 2e-5
+    assert subspace_distance(out["mixed"][0], out["fp64"][0]) < 1e-3
