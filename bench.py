@@ -32,6 +32,12 @@ sys.path.insert(0, ROOT)
 
 METRIC = "s/SCF-iter Si216 CheFSI: mixed vs plain FP64 on B200 at ΔE≤1e-5 Ha/atom; HBM GB/s"
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one cheb_pipe_kernel launch per
+# grid-point x state update, from an ncu capture of the Si64 case (60^3 grid, 160 states):
+# 447.7 MB (FP32) and 927.2 MB (FP64) per launch.  Whole planes stream through the same band
+# geometry at every size, so the traffic of a launch scales with the updates it processes.
+TRAFFIC_PER_UPDATE = {"mixed": 447.7e6 / (216000 * 160), "fp64": 927.2e6 / (216000 * 160)}
+
 CONFIGS = {
     # name: (reps, grid, nstates, degree, displace)
     "si216": (3, 90, 520, 20, 0.02),
@@ -356,7 +362,9 @@ def main():
             "speedup_vs_fp64" if args.precision == "mixed" else "speedup_vs_mixed": t_other / t_main,
             "accuracy": acc,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": None, "kernel": "cheb_step_kernel (fused stencil+Veff+recurrence)",
+                         "traffic": TRAFFIC_PER_UPDATE[args.precision] * ctx.nd * nst,
+                         "traffic_source": "ncu capture of the Si64 case scaled by updates per launch",
+                         "kernel": "cheb_pipe_kernel (fused stencil + Veff + three-term recurrence)",
                          "ms_per_launch": ms.value, "ms_per_step_with_nonlocal": ms_nl.value,
                          "peak_kind": peak_kind},
             "clocks": clk.summary(),
