@@ -182,6 +182,15 @@ LYNX_API int lynx_occupations(const double* eigs, int n, double ef, double beta,
 LYNX_API int lynx_time_filter_step(lynx_ctx* ctx, const double* veff, int ncol, int precision, int with_nonlocal,
                                    int reps, double* ms_per_step);
 
+/* hpsi += Vnl psi, as lynx_nonlocal_apply, but with no device allocation: the projector
+ * coefficients live in a fixed 8 MiB device array inside the library (total projectors x ncol
+ * rounded up to 32, in doubles, must fit, else LYNX_ERR_BAD_ARG).  No counterpart in the
+ * reference: its GPU path sizes d_alpha once for Nband columns in Hamiltonian::setup_gpu
+ * (src/operators/Hamiltonian.cu:473) and has no per-call variant.  The array is shared by all
+ * contexts on a device, so calls overlapping in time race; the first call on a device does
+ * one-time set-up and should come before any stream capture.  Real (Gamma-point) FP64 only. */
+LYNX_API int lynx_nonlocal_apply_noalloc(lynx_ctx* ctx, const double* psi, double* hpsi, int ncol, int ld);
+
 /* Number of kernel launches this library issued since the last reset (diagnostic counter). */
 LYNX_API long long lynx_launch_count(int reset);
 

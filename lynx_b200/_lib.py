@@ -60,6 +60,7 @@ _SIGNATURES = {
     "lynx_hamiltonian_apply": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double]),
     "lynx_hamiltonian_apply_kpt": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double]),
     "lynx_nonlocal_apply": (_c_int, [_p, _p, _p, _c_int, _c_int]),
+    "lynx_nonlocal_apply_noalloc": (_c_int, [_p, _p, _p, _c_int, _c_int]),
     "lynx_nonlocal_apply_kpt": (_c_int, [_p, _p, _p, _c_int, _c_int]),
     "lynx_chebyshev_filter": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _c_int]),
     "lynx_chebyshev_filter_kpt": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _c_int]),

@@ -1536,3 +1536,69 @@ int lynx_occupations(const double* eigs, int n, double ef, double beta, int smea
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Nonlocal apply without device allocation.
+//
+// lynx_nonlocal_apply keeps its projector coefficients alpha in a context buffer that grows
+// with cudaMalloc on first use.  Some callers must not allocate at that point: a host program
+// that reserves its whole device-memory budget up front (cudaMalloc then fails or evicts its
+// own pool), and code that interleaves the apply with latency-critical work on other streams
+// (cudaFree synchronises the whole device, and cudaMalloc may).  This entry point keeps alpha
+// in a fixed file-scope device array instead, so a call issues only kernel launches.
+//
+// Limits: alpha needs total_proj x ncolp doubles (ncolp = ncol rounded up to 32); requests
+// larger than kNoAllocScratchBytes are rejected with LYNX_ERR_BAD_ARG (split the columns).
+// The scratch array is shared by every context on a device: calls that overlap in time (two
+// streams or two host threads on one device) race on it and must be serialised by the caller.
+// The first call on a device resolves the array's address (cudaGetSymbolAddress, which also
+// loads the module) and should be made once before any stream capture is begun.  Nothing in
+// the scratch needs to start at zero: the gather writes every alpha element the scatter reads.
+// ---------------------------------------------------------------------------------------------
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB = 1 Mi doubles
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+constexpr int kNoAllocMaxDevices = 64;
+std::atomic<void*> g_noalloc_addr[kNoAllocMaxDevices];
+
+int noalloc_scratch(int device, void** out) {
+    if (device < 0 || device >= kNoAllocMaxDevices) {
+        set_error("device index %d out of range for the no-allocation scratch", device);
+        return LYNX_ERR_BAD_ARG;
+    }
+    void* p = g_noalloc_addr[device].load(std::memory_order_acquire);
+    if (!p) {
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaGetSymbolAddress(no-allocation scratch) failed: %s", cudaGetErrorString(e));
+            return LYNX_ERR_CUDA;
+        }
+        g_noalloc_addr[device].store(p, std::memory_order_release);
+    }
+    *out = p;
+    return LYNX_OK;
+}
+}  // namespace
+
+extern "C" int lynx_nonlocal_apply_noalloc(lynx_ctx* c, const double* psi, double* hpsi, int ncol, int ld) {
+    LYNX_CHECK_ARG(c && psi && hpsi, "null pointer");
+    LYNX_CHECK_ARG(ncol > 0, "ncol must be positive");
+    const long long l = ld > 0 ? ld : c->Nd;
+    LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
+    if (!c->has_nl) return LYNX_OK;
+    const int ncolp = ((ncol + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
+    const size_t need = sizeof(double) * (size_t)c->nl.total_proj * (size_t)ncolp;
+    if (need > kNoAllocScratchBytes) {
+        set_error("no-allocation nonlocal apply needs %zu bytes of scratch for %d projectors x %d columns; "
+                  "the limit is %zu bytes: apply fewer columns per call",
+                  need, c->nl.total_proj, ncol, kNoAllocScratchBytes);
+        return LYNX_ERR_BAD_ARG;
+    }
+    LYNX_CUDA_TRY(cudaSetDevice(c->device));
+    void* scratch = nullptr;
+    LYNX_TRY(noalloc_scratch(c->device, &scratch));
+    double* alpha = static_cast<double*>(scratch);
+    LYNX_TRY(launch_nl_gather<double>(c->nl, psi, l, ncol, alpha, ncolp, c->dV, c->stream));
+    return launch_nl_scatter<double, double>(c->nl, hpsi, l, ncol, alpha, ncolp, 1.0, c->stream);
+}
