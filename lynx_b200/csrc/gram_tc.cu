@@ -353,6 +353,27 @@ int make_map(CUtensorMap* m, const int8_t* ptr, long long ldk, int rows) {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// 2-D int8 tensor [rows][ldk] with K extent kext <= ldk (reads past kext are zero-filled).
+int make_map_k(CUtensorMap* m, const int8_t* ptr, long long ldk, long long kext, long long rows) {
+    auto enc = get_encode();
+    if (!enc) {
+        set_error("cuTensorMapEncodeTiled is not available");
+        return LYNX_ERR_CUDA;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)kext, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ldk};
+    cuuint32_t box[2] = {BK, BM};
+    cuuint32_t es[2] = {1, 1};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<int8_t*>(ptr), dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
 }  // namespace
 
 GramPlan gram_plan(long long rows, int n) {
@@ -375,6 +396,259 @@ GramPlan gram_plan(long long rows, int n) {
     p.work_bytes = 6 * p.slice_bytes + 2 * p.exp_bytes + p.ws_bytes;
     return p;
 }
+
+namespace {
+
+// ---------------------------------------------------------------------------------------------
+// Subspace rotation psi = Y W on the tensor cores (src/solvers/EigenSolver.cpp:674-681), same
+// exact-slice scheme as the Gram products.  The states of Y are first rescaled by powers of two
+// taken from the overlap diagonal (Y~ = Y 2^-d, W~ = 2^d W, so Y~ W~ = Y W and the rows of Y~
+// hold numbers of comparable size); each grid-point row of Y~ is then sliced with its own
+// exponent e_r over all states, each column of W~ with its own exponent f_j.  The contraction
+// runs over the states (K = N), so one int32 accumulation per level covers it exactly, and
+//     psi[r][j] = 2^(e_r + f_j) (acc2 2^-14 + acc3 2^-21 + acc4 2^-28)
+// is formed exactly in FP64 and stored straight into the caller's (unpadded) FP64 layout.
+// The three-slice representation (relative 2^-20 of the row / column maximum, unbiased) makes
+// the rotation as accurate as an FP32 GEMM of the same depth.
+// ---------------------------------------------------------------------------------------------
+struct RotArgs {
+    int N;            // states (K extent and output columns)
+    int nsteps;       // K stages of BK
+    int ntn;          // output column tiles
+    long long rows;   // rows of the padded Y block
+    int nx, nxp;      // row padding: r = x + nxp * rest, x < nx valid
+    const int* erow;  // [rows] row exponents
+    const int* fcol;  // [N] column exponents
+    double* psi;      // output, column stride ldp, unpadded rows
+    long long ldp;
+    int* err;
+};
+
+__global__ void __launch_bounds__(128, 1)
+    rot_i8_kernel(const __grid_constant__ CUtensorMap tA1, const __grid_constant__ CUtensorMap tA2,
+                  const __grid_constant__ CUtensorMap tA3, const __grid_constant__ CUtensorMap tB1,
+                  const __grid_constant__ CUtensorMap tB2, const __grid_constant__ CUtensorMap tB3,
+                  const RotArgs g) {
+    extern __shared__ __align__(1024) unsigned char gsm[];
+    unsigned char* base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(gsm) + 1023) & ~static_cast<uintptr_t>(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* done = empty + STAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tm = blockIdx.x / g.ntn, tn = blockIdx.x % g.ntn;  // column tiles of one row tile adjacent
+    const int m0 = tm * BM, n0 = tn * BN;
+    const CUtensorMap* mA[NSLICE] = {&tA1, &tA2, &tA3};
+    const CUtensorMap* mB[NSLICE] = {&tB1, &tB2, &tB3};
+    auto tileA = [&](int s, int q) { return base + s * STAGE_BYTES + q * TILE_BYTES; };
+    auto tileB = [&](int s, int q) { return base + s * STAGE_BYTES + (NSLICE + q) * TILE_BYTES; };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    bool ok = true;
+    if (warp == 0 && lane == 0) {
+        for (int k = 0; k < g.nsteps; ++k) {
+            const int s = k % STAGES, u = k / STAGES;
+            if (u > 0 && !mbar_wait(&empty[s], (uint32_t)((u - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            mbar_expect_tx(&full[s], STAGE_BYTES);
+            const int x = k * BK;
+#pragma unroll
+            for (int q = 0; q < NSLICE; ++q) {
+                tma_load_2d(tileA(s, q), mA[q], x, m0, &full[s]);
+                tma_load_2d(tileB(s, q), mB[q], x, n0, &full[s]);
+            }
+        }
+    } else if (warp == 1 && lane == 0) {
+        for (int k = 0; k < g.nsteps; ++k) {
+            const int s = k % STAGES, u = k / STAGES;
+            if (!mbar_wait(&full[s], (uint32_t)(u & 1))) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            uint64_t a[NSLICE], b[NSLICE];
+#pragma unroll
+            for (int q = 0; q < NSLICE; ++q) {
+                a[q] = sw128_desc(smem_u32(tileA(s, q)));
+                b[q] = sw128_desc(smem_u32(tileB(s, q)));
+            }
+#pragma unroll
+            for (int kk = 0; kk < BK / 32; ++kk) {
+                if (k * BK + kk * 32 >= g.N) break;  // K sub-steps past the last state hold zeros only
+                const uint64_t off = (uint64_t)(kk * 32) >> 4;
+                const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+                mma_i8(tmem + 0, a[0] + off, b[0] + off, acc);
+                mma_i8(tmem + 128, a[0] + off, b[1] + off, acc);
+                mma_i8(tmem + 128, a[1] + off, b[0] + off, 1u);
+                mma_i8(tmem + 256, a[0] + off, b[2] + off, acc);
+                mma_i8(tmem + 256, a[1] + off, b[1] + off, 1u);
+                mma_i8(tmem + 256, a[2] + off, b[0] + off, 1u);
+            }
+            mma_commit(&empty[s]);
+        }
+        mma_commit(done);
+    }
+    __syncwarp();
+    if (!mbar_wait(done, 0)) ok = false;
+    ok = __all_sync(0xffffffffu, ok);
+    tc_fence_after();
+    if (ok) {
+        const long long row = (long long)m0 + warp * 32 + lane;
+        long long ridx = -1;
+        int er = 0;
+        if (row < g.rows) {
+            const long long xr = row % g.nxp, rest = row / g.nxp;
+            if (xr < g.nx) ridx = xr + (long long)g.nx * rest;
+            er = g.erow[row];
+        }
+        const uint32_t lb = (uint32_t)(warp * 32) << 16;
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            uint32_t r2[16], r3[16], r4[16];
+            tmem_ld16(tmem + lb + (uint32_t)c0, r2);
+            tmem_ld16(tmem + lb + 128u + (uint32_t)c0, r3);
+            tmem_ld16(tmem + lb + 256u + (uint32_t)c0, r4);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (ridx >= 0) {
+#pragma unroll
+                for (int t = 0; t < 16; ++t) {
+                    const int j = n0 + c0 + t;
+                    if (j < g.N) {
+                        const double x = (double)(int)r2[t] * 0x1p-14 + (double)(int)r3[t] * 0x1p-21 +
+                                         (double)(int)r4[t] * 0x1p-28;
+                        g.psi[(long long)j * g.ldp + ridx] = ldexp(x, er + g.fcol[j]);
+                    }
+                }
+            }
+        }
+    }
+    if (!ok && lane == 0) atomicExch(g.err, 1);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+    }
+}
+
+// Column exponents d_i of Y from the overlap diagonal (Ms_ii = dV |y_i|^2): 2^d_i ~ |y_i|.
+__global__ void colexp_kernel(const double* __restrict__ Ms, int n, int* __restrict__ d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const double v = Ms[i + (long long)i * n];
+        d[i] = (v > 0.0) ? ilogb(sqrt(v)) : 0;
+    }
+}
+
+// Rows of Y 2^-d -> exponent e_r and three int8 slices a_q[r][i] (state index contiguous,
+// row stride ldk >= N, states N..ldk-1 written as zero).  CTA = 32 consecutive rows, all
+// states staged in shared memory [state][row] (row stride 33).
+__global__ void __launch_bounds__(256)
+    slice_rows_kernel(int8_t* __restrict__ a1, int8_t* __restrict__ a2, int8_t* __restrict__ a3, long long ldk,
+                      int* __restrict__ erow, const float* __restrict__ y, long long ldy, long long rows, int N,
+                      const int* __restrict__ dcol) {
+    extern __shared__ __align__(16) float tsm[];  // [N][33]
+    __shared__ int es[32];
+    const long long r0 = (long long)blockIdx.x * 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = w; i < N; i += 8) {
+        const long long r = r0 + lane;
+        tsm[i * 33 + lane] = (r < rows) ? ldexpf(y[(long long)i * ldy + r], -dcol[i]) : 0.0f;
+    }
+    __syncthreads();
+    for (int rr = w; rr < 32; rr += 8) {
+        float m = 0.0f;
+        for (int i = lane; i < N; i += 32) m = fmaxf(m, fabsf(tsm[i * 33 + rr]));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        int E = 0;
+        if (m > 0.0f) frexpf(m, &E);
+        if (lane == 0) es[rr] = (m > 0.0f) ? E + 1 : 0;
+    }
+    __syncthreads();
+    for (int rr = w; rr < 32; rr += 8) {
+        const long long r = r0 + rr;
+        if (r >= rows) continue;
+        const int e = es[rr];
+        if (lane == 0) erow[r] = e;
+        for (int i0 = 4 * lane; i0 < ldk; i0 += 128) {
+            char4 o1, o2, o3;
+            int8_t* p1 = reinterpret_cast<int8_t*>(&o1);
+            int8_t* p2 = reinterpret_cast<int8_t*>(&o2);
+            int8_t* p3 = reinterpret_cast<int8_t*>(&o3);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = i0 + q;
+                float t = (i < N) ? ldexpf(tsm[i * 33 + rr], 7 - e) : 0.0f;
+                const float a = rintf(t);
+                t = (t - a) * 128.0f;
+                const float b = rintf(t);
+                t = (t - b) * 128.0f;
+                const float c = rintf(t);
+                p1[q] = (int8_t)(int)a;
+                p2[q] = (int8_t)(int)b;
+                p3[q] = (int8_t)(int)c;
+            }
+            *reinterpret_cast<char4*>(a1 + r * ldk + i0) = o1;
+            *reinterpret_cast<char4*>(a2 + r * ldk + i0) = o2;
+            *reinterpret_cast<char4*>(a3 + r * ldk + i0) = o3;
+        }
+    }
+}
+
+// Columns of 2^d W (FP64, column-major N x N) -> exponent f_j and three int8 slices b_q[j][i].
+__global__ void __launch_bounds__(128)
+    slice_w_kernel(int8_t* __restrict__ b1, int8_t* __restrict__ b2, int8_t* __restrict__ b3, long long ldk,
+                   int* __restrict__ fcol, const double* __restrict__ W, int N, const int* __restrict__ dcol) {
+    __shared__ double red[4];
+    const int j = blockIdx.x;
+    const double* col = W + (long long)j * N;
+    double m = 0.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) m = fmax(m, fabs(ldexp(col[i], dcol[i])));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = fmax(fmax(red[0], red[1]), fmax(red[2], red[3]));
+    int E = 0;
+    if (m > 0.0) frexp(m, &E);
+    const int f = (m > 0.0) ? E + 1 : 0;
+    if (threadIdx.x == 0) fcol[j] = f;
+    for (int i = threadIdx.x; i < ldk; i += blockDim.x) {
+        double t = (i < N) ? ldexp(col[i], dcol[i] + 7 - f) : 0.0;
+        const double a = rint(t);
+        t = (t - a) * 128.0;
+        const double b = rint(t);
+        t = (t - b) * 128.0;
+        const double c = rint(t);
+        b1[(long long)j * ldk + i] = (int8_t)(int)a;
+        b2[(long long)j * ldk + i] = (int8_t)(int)b;
+        b3[(long long)j * ldk + i] = (int8_t)(int)c;
+    }
+}
+
+}  // namespace
 
 int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows, int n, double dV,
                    const GramPlan& p, void* work, size_t work_bytes, double* Ms, double* Hs, int* err,
@@ -421,6 +695,77 @@ int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("Gram kernel launch failed: %s", cudaGetErrorString(e));
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+RotPlan rot_plan(long long rows, int n) {
+    RotPlan p;
+    p.ldk = ((n + 15) / 16) * 16;
+    p.a_bytes = align256((size_t)rows * p.ldk);
+    p.b_bytes = align256((size_t)n * p.ldk);
+    p.erow_bytes = align256((size_t)rows * sizeof(int));
+    p.col_bytes = align256((size_t)n * sizeof(int));
+    p.work_bytes = 3 * p.a_bytes + 3 * p.b_bytes + p.erow_bytes + 2 * p.col_bytes;
+    p.smem_rows = (size_t)n * 33 * sizeof(float);
+    return p;
+}
+
+bool rot_supported(int n) { return (size_t)n * 33 * sizeof(float) <= 200 * 1024; }
+
+int launch_colexp(const double* Ms, int n, void* work, const RotPlan& p, long long rows, cudaStream_t st) {
+    unsigned char* w = static_cast<unsigned char*>(work);
+    int* dcol = reinterpret_cast<int*>(w + 3 * p.a_bytes + 3 * p.b_bytes + p.erow_bytes);
+    colexp_kernel<<<(n + 127) / 128, 128, 0, st>>>(Ms, n, dcol);
+    count_launch();
+    return LYNX_OK;
+}
+
+int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp, const double* W, int n,
+                  const RotPlan& p, void* work, size_t work_bytes, double* psi, long long ldp, int* err,
+                  cudaStream_t st) {
+    if (work_bytes < p.work_bytes || (reinterpret_cast<uintptr_t>(work) & 255) || !rot_supported(n)) {
+        set_error("rotation workspace too small or misaligned, or too many states for the tensor-core rotation");
+        return LYNX_ERR_BAD_ARG;
+    }
+    unsigned char* w = static_cast<unsigned char*>(work);
+    int8_t* a[3];
+    int8_t* b[3];
+    for (int q = 0; q < 3; ++q) a[q] = reinterpret_cast<int8_t*>(w + q * p.a_bytes);
+    for (int q = 0; q < 3; ++q) b[q] = reinterpret_cast<int8_t*>(w + 3 * p.a_bytes + q * p.b_bytes);
+    int* erow = reinterpret_cast<int*>(w + 3 * p.a_bytes + 3 * p.b_bytes);
+    int* dcol = reinterpret_cast<int*>(w + 3 * p.a_bytes + 3 * p.b_bytes + p.erow_bytes);
+    int* fcol = dcol + p.col_bytes / sizeof(int);
+    LYNX_CUDA_TRY(cudaFuncSetAttribute(slice_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)p.smem_rows));
+    slice_rows_kernel<<<(unsigned)((rows + 31) / 32), 256, p.smem_rows, st>>>(a[0], a[1], a[2], p.ldk, erow, Y, ldy,
+                                                                               rows, n, dcol);
+    slice_w_kernel<<<n, 128, 0, st>>>(b[0], b[1], b[2], p.ldk, fcol, W, n, dcol);
+    count_launch(2);
+    CUtensorMap m[6];
+    for (int q = 0; q < 3; ++q) LYNX_TRY(make_map_k(&m[q], a[q], p.ldk, n, rows));
+    for (int q = 0; q < 3; ++q) LYNX_TRY(make_map_k(&m[3 + q], b[q], p.ldk, n, n));
+    RotArgs g;
+    g.N = n;
+    g.nsteps = (n + BK - 1) / BK;
+    g.ntn = (n + BN - 1) / BN;
+    g.rows = rows;
+    g.nx = nx;
+    g.nxp = nxp;
+    g.erow = erow;
+    g.fcol = fcol;
+    g.psi = psi;
+    g.ldp = ldp;
+    g.err = err;
+    const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
+    LYNX_CUDA_TRY(cudaFuncSetAttribute(rot_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long long ntm = (rows + BM - 1) / BM;
+    rot_i8_kernel<<<(unsigned)(ntm * g.ntn), 128, smem, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], g);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("rotation kernel launch failed: %s", cudaGetErrorString(e));
         return LYNX_ERR_CUDA;
     }
     return LYNX_OK;

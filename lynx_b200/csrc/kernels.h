@@ -48,6 +48,20 @@ int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows
                    const GramPlan& p, void* work, size_t work_bytes, double* Ms, double* Hs, int* err,
                    cudaStream_t st);
 
+// Subspace rotation psi = Y W on the tensor cores (exact int8 slices, FP64 output written into
+// an unpadded layout with column stride ldp); gram_tc.cu.  launch_colexp must run on the
+// overlap Ms (before its Cholesky factorisation) to fix the per-state scaling.
+struct RotPlan {
+    long long ldk;  // row stride (bytes) of the slice arrays, >= N
+    size_t a_bytes, b_bytes, erow_bytes, col_bytes, work_bytes, smem_rows;
+};
+RotPlan rot_plan(long long rows, int n);
+bool rot_supported(int n);
+int launch_colexp(const double* Ms, int n, void* work, const RotPlan& p, long long rows, cudaStream_t st);
+int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp, const double* W, int n,
+                  const RotPlan& p, void* work, size_t work_bytes, double* psi, long long ldp, int* err,
+                  cudaStream_t st);
+
 // Launches issued by the library (diagnostic counter, incremented by every launcher).
 void count_launch(int n = 1);
 
@@ -56,8 +70,15 @@ void count_launch(int n = 1);
 namespace lynxb {
 
 // Device copy of the nonlocal projector tables (see nonlocal.cuh for the layout).
+constexpr int kNLMaxColors = 16;  // colour classes the register-tiled scatter accepts
+
 struct NLDev {
     int n_atom = 0, n_img = 0, n_pts = 0, max_np = 0, total_proj = 0;
+    // Images in colour classes with pairwise disjoint grid points (n_colors = 0: not coloured,
+    // the pull-style scatter is used); class k is color_img[color_off[k] .. color_off[k+1]).
+    int n_colors = 0;
+    int color_off[kNLMaxColors + 1] = {};
+    int* color_img = nullptr;
     int* atom_img_ptr = nullptr;
     int* atom_img_list = nullptr;
     int* atom_nproj = nullptr;

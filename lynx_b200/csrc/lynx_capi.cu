@@ -167,6 +167,7 @@ struct lynx_ctx {
     DevBuf vpad64, vpad32;  // Veff in the padded row layouts of the pipelined stencil
     DevBuf errflag;         // set by a kernel whose bounded wait gave up
     DevBuf gwork;           // slices, exponents and split partials of the tensor-core Gram
+    DevBuf rwork;           // slices and exponents of the tensor-core rotation
     bool no_tc_gram = false;  // diagnostic switch: FP64 library products for the mixed path
     // nonlocal tables re-indexed for padded row layouts: nxp -> tables
     std::map<int, NLDev> nl_layouts;
@@ -653,12 +654,11 @@ int finish_rr(lynx_ctx* c, int N, double* eig_host) {
 
 // Subspace part of the Rayleigh-Ritz step, given Ms = dV Y^T Y and Hs = dV Y^T HY in c->Ms /
 // c->Hs (Ms: at least the upper triangle): Hs' = R^-T sym(Hs) R^-1 with R^T R = Ms,
-// eigenpairs of Hs', W = R^-1 Q, psi = Yrot W.  Yrot: FP64 block with Nd rows.
-int rr_subspace_real(lynx_ctx* c, const double* Yrot, long long ldY, double* psi, long long ldp, int N,
-                     double* eig_host) {
+// eigenpairs of Hs' (values into c->eigd), W = R^-1 Q left in c->Hs.  Asynchronous.
+int rr_small_real(lynx_ctx* c, int N) {
     double* Ms = c->Ms.as<double>();
     double* Hs = c->Hs.as<double>();
-    const double one = 1.0, zero = 0.0;
+    const double one = 1.0;
     {
         dim3 b(16, 16), g((N + 15) / 16, (N + 15) / 16);
         symmetrize_kernel<<<g, b, 0, c->stream>>>(Hs, N);
@@ -682,7 +682,16 @@ int rr_subspace_real(lynx_ctx* c, const double* Yrot, long long ldY, double* psi
                                   c->eigd.as<double>(), c->solver_work.as<double>(), lw, info + 1));
     CUBLAS_TRY(cublasDtrsm(c->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
                            N, N, &one, Ms, N, Hs, N));
-    CUBLAS_TRY(cublasDgemm(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, c->Nd, N, N, &one, Yrot, ldY, Hs, N, &zero, psi, ldp));
+    return LYNX_OK;
+}
+
+// rr_small_real, then psi = Yrot W by cuBLAS DGEMM (Yrot: FP64 block with Nd rows).
+int rr_subspace_real(lynx_ctx* c, const double* Yrot, long long ldY, double* psi, long long ldp, int N,
+                     double* eig_host) {
+    LYNX_TRY(rr_small_real(c, N));
+    const double one = 1.0, zero = 0.0;
+    CUBLAS_TRY(cublasDgemm(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, c->Nd, N, N, &one, Yrot, ldY, c->Hs.as<double>(), N,
+                           &zero, psi, ldp));
     return finish_rr(c, N, eig_host);
 }
 
@@ -709,8 +718,9 @@ int rayleigh_ritz_real(lynx_ctx* c, const double* Y, long long ldY, const double
     return rr_subspace_real(c, Y, ldY, psi, ldp, N, eig_host);
 }
 
-// Mixed precision, real: Gram products of the FP32 blocks on the tensor cores (exact int8
-// slice products, FP64 combination), subspace algebra in FP64, rotation of an FP64 copy of Y.
+// Mixed precision, real: Gram products and rotation of the FP32 blocks on the tensor cores
+// (exact int8 slice products, FP64 combination), subspace algebra in FP64.  More states than
+// the rotation kernel stages take the rotation by DGEMM on an FP64 copy of Y.
 int rayleigh_ritz_mixed_real(lynx_ctx* c, const float* Y32, const float* HY32, long long ldb, int nxp, double* psi,
                              long long ldp, int N, double* eig_host) {
     LYNX_TRY(rr_alloc_small(c, N, sizeof(double)));
@@ -719,6 +729,16 @@ int rayleigh_ritz_mixed_real(lynx_ctx* c, const float* Y32, const float* HY32, l
     if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
     LYNX_TRY(launch_gram_i8(Y32, HY32, ldb, ldb, N, c->dV, plan, c->gwork.p, c->gwork.bytes, c->Ms.as<double>(),
                             c->Hs.as<double>(), c->errflag.as<int>(), c->stream));
+    if (rot_supported(N)) {
+        // rotation on the tensor cores, straight from the FP32 block into the caller's psi
+        const RotPlan rp = rot_plan(ldb, N);
+        LYNX_TRY(c->rwork.ensure(rp.work_bytes));
+        LYNX_TRY(launch_colexp(c->Ms.as<double>(), N, c->rwork.p, rp, ldb, c->stream));
+        LYNX_TRY(rr_small_real(c, N));
+        LYNX_TRY(launch_rot_i8(Y32, ldb, ldb, c->nx, nxp, c->Hs.as<double>(), N, rp, c->rwork.p, c->rwork.bytes, psi,
+                               ldp, c->errflag.as<int>(), c->stream));
+        return finish_rr(c, N, eig_host);
+    }
     const long long Nd = c->Nd;
     LYNX_TRY(c->cvt[0].ensure(sizeof(double) * (size_t)Nd * N));
     LYNX_TRY(repack<double, float>(c, c->cvt[0].as<double>(), c->nx, Nd, Y32, nxp, ldb, N));
@@ -1132,6 +1152,7 @@ int lynx_destroy(lynx_ctx* c) {
     c->vpad32.release();
     c->errflag.release();
     c->gwork.release();
+    c->rwork.release();
     for (auto& b : c->nl_layout_bufs) b.release();
     if (c->cublas) cublasDestroy(c->cublas);
     if (c->cusolver) cusolverDnDestroy(c->cusolver);
@@ -1244,6 +1265,36 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
         ent_loc[s] = owner_loc[k];
     }
     pt_ptr.push_back((int)tot);
+    // Greedy colouring of the images: two images that share a grid point get different
+    // colours, so the register-tiled scatter can run one colour class per launch with a single
+    // writer per output element.  Images are coloured in index order (deterministic).
+    std::vector<int> color(n_img, -1), color_img;
+    int n_colors = 0;
+    {
+        std::vector<std::vector<int>> adj(n_img);
+        for (size_t p = 0; p + 1 < pt_ptr.size(); ++p)
+            for (int u = pt_ptr[p]; u < pt_ptr[p + 1]; ++u)
+                for (int v = u + 1; v < pt_ptr[p + 1]; ++v)
+                    if (ent_img[u] != ent_img[v]) {
+                        adj[ent_img[u]].push_back(ent_img[v]);
+                        adj[ent_img[v]].push_back(ent_img[u]);
+                    }
+        for (int i = 0; i < n_img; ++i) {
+            unsigned long long used = 0;
+            for (int j : adj[i])
+                if (color[j] >= 0 && color[j] < 64) used |= 1ull << color[j];
+            const int cl = (~used) ? __builtin_ctzll(~used) : 64;
+            color[i] = cl;
+            n_colors = std::max(n_colors, cl + 1);
+        }
+        if (n_colors <= kNLMaxColors) {
+            for (int k = 0; k < n_colors; ++k)
+                for (int i = 0; i < n_img; ++i)
+                    if (color[i] == k) color_img.push_back(i);
+        } else {
+            n_colors = 0;
+        }
+    }
     std::vector<float> chi32(totchi);
     for (long long k = 0; k < totchi; ++k) chi32[k] = (float)chi[k];
     // upload
@@ -1255,7 +1306,7 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
         *dst = b.p;
         return LYNX_OK;
     };
-    c->nl_bufs.reserve(20);
+    c->nl_bufs.reserve(24);
     NLDev& d = c->nl;
     d.n_atom = n_atom;
     d.n_img = n_img;
@@ -1281,6 +1332,15 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
     LYNX_TRY(up(pt_ptr.data(), pt_ptr.size() * 4, (void**)&d.pt_ptr));
     LYNX_TRY(up(ent_img.data(), ent_img.size() * 4, (void**)&d.ent_img));
     LYNX_TRY(up(ent_loc.data(), ent_loc.size() * 4, (void**)&d.ent_loc));
+    d.n_colors = n_colors;
+    if (n_colors > 0) {
+        for (int k = 0, o = 0; k < n_colors; ++k) {
+            d.color_off[k] = o;
+            for (int i = 0; i < n_img; ++i) o += (color[i] == k);
+            d.color_off[k + 1] = o;
+        }
+        LYNX_TRY(up(color_img.data(), color_img.size() * 4, (void**)&d.color_img));
+    }
     c->img_shift.assign(img_shift, img_shift + 3 * n_img);
     c->h_gpos.assign(gpos, gpos + tot);
     c->h_pt_grid = pt_grid;

@@ -189,4 +189,244 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Register-tiled kernels for real (Gamma-point) data, T = float or double.
+//
+// gather2: CTA = (physical atom, 64 columns), 256 threads.  Point tiles of 64 sphere points are
+// staged in shared memory: x as [point][column] with the 4-column groups XOR-swizzled by the
+// point index (conflict-free stores from point-major loads and float4/double2 reads), chi as
+// [point][two projector groups padded to 16 bytes].  Lane = (column group cg of 4 columns,
+// projector group pg of NPG projectors), so every thread keeps 4 x NPG accumulators; the 8
+// warps split the points of a tile and their partial sums are added in a fixed binary tree
+// at the end (deterministic).
+//
+// scatter2: CTA = (image, 64 columns), 256 threads; images are launched one colour class at a
+// time, and no two images of a class touch the same grid point, so every output element has
+// one writer per launch and the summation order is fixed.  Warp w owns columns 8w..8w+7,
+// lane owns 2 points of a 64-point tile; chi is staged [projector][point] and the atom's
+// alpha block [projector][column] is read as broadcasts.
+// ---------------------------------------------------------------------------------------------
+constexpr int kNL2Cols = 64;  // columns per CTA of gather2 / scatter2
+constexpr int kNL2Pts = 64;   // points per staged tile
+
+template <typename T>
+__device__ __forceinline__ void load_vec4(const T* p, T (&v)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(p);
+        v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+    } else {
+        const double2 q0 = *reinterpret_cast<const double2*>(p);
+        const double2 q1 = *reinterpret_cast<const double2*>(p + 2);
+        v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void store_vec4(T* p, const T (&v)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+        *reinterpret_cast<double2*>(p + 2) = make_double2(v[2], v[3]);
+    }
+}
+
+template <typename T, int NPG>
+struct Gather2Geom {
+    static constexpr int VW = 16 / sizeof(T);
+    static constexpr int NPGP = (NPG + VW - 1) / VW * VW;  // projector group stride, 16-byte multiple
+    static constexpr int CSP = 2 * NPGP;                   // chi row stride
+    static constexpr size_t xs_elems = (size_t)kNL2Pts * kNL2Cols;
+    static constexpr size_t cs_elems = (size_t)kNL2Pts * CSP;
+    static constexpr size_t red_elems = (size_t)4 * 32 * 4 * NPG;  // 4 warps x 32 lanes x accumulators
+    static constexpr size_t smem_bytes =
+        sizeof(T) * ((xs_elems + cs_elems) > red_elems ? (xs_elems + cs_elems) : red_elems);
+};
+
+template <typename T, int NPG>
+__global__ void __launch_bounds__(256)
+    nl_gather2_kernel(const T* __restrict__ x, long long ld, int ncol, int ncolp, NLView tab, T* __restrict__ alpha,
+                      double dV) {
+    using Geo = Gather2Geom<T, NPG>;
+    constexpr int NB = kNL2Cols, G = kNL2Pts, NPGP = Geo::NPGP, CSP = Geo::CSP;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T* xs = reinterpret_cast<T*>(smraw);  // [G][NB], 4-column groups swizzled by (g & 7)
+    T* cs = xs + Geo::xs_elems;           // [G][CSP]
+    const T* chi = reinterpret_cast<const T*>(tab.chi);
+    const int a = blockIdx.x;
+    const int n0 = blockIdx.y * NB;
+    const int np = tab.atom_nproj[a];
+    const int poff = tab.atom_poff[a];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int cg = lane & 15, pg = lane >> 4;
+    T acc[4][NPG];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int m = 0; m < NPG; ++m) acc[k][m] = T(0);
+    for (int ii = tab.atom_img_ptr[a]; ii < tab.atom_img_ptr[a + 1]; ++ii) {
+        const int im = tab.atom_img_list[ii];
+        const int ndc = tab.img_ndc[im];
+        const int* gp = tab.gpos + tab.img_goff[im];
+        const T* ch = chi + tab.img_chi_off[im];
+        for (int g0 = 0; g0 < ndc; g0 += G) {
+            const int gl = min(G, ndc - g0);
+            __syncthreads();
+#pragma unroll
+            for (int pp = 0; pp < 2; ++pp) {
+                const int g = lane + 32 * pp;
+                const bool okg = g < gl;
+                const long long base = okg ? (long long)gp[g0 + g] : 0;
+#pragma unroll
+                for (int qq = 0; qq < 2; ++qq) {
+                    const int q = w + 8 * qq;
+                    T v[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int col = n0 + 4 * q + k;
+                        v[k] = (okg && col < ncol) ? x[base + (long long)col * ld] : T(0);
+                    }
+                    store_vec4(xs + g * NB + 4 * (q ^ (g & 7)), v);
+                }
+            }
+            for (int e = tid; e < G * CSP; e += 256) {
+                const int g = e % G, sl = e / G;
+                const int gq = sl / NPGP, m = sl % NPGP;
+                const int j = gq * NPG + m;
+                cs[g * CSP + sl] = (g < gl && m < NPG && j < np) ? ch[(long long)j * ndc + g0 + g] : T(0);
+            }
+            __syncthreads();
+            for (int g = w; g < gl; g += 8) {
+                T xv[4];
+                load_vec4(xs + g * NB + 4 * (cg ^ (g & 7)), xv);
+                const T* cp = cs + g * CSP + pg * NPGP;
+                T cv[NPGP];
+                if constexpr (sizeof(T) == 4) {
+#pragma unroll
+                    for (int m = 0; m < NPGP; m += 4) {
+                        const float4 q = *reinterpret_cast<const float4*>(cp + m);
+                        cv[m] = q.x;
+                        cv[m + 1] = q.y;
+                        cv[m + 2] = q.z;
+                        cv[m + 3] = q.w;
+                    }
+                } else {
+#pragma unroll
+                    for (int m = 0; m < NPGP; m += 2) {
+                        const double2 q = *reinterpret_cast<const double2*>(cp + m);
+                        cv[m] = q.x;
+                        cv[m + 1] = q.y;
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+#pragma unroll
+                    for (int m = 0; m < NPG; ++m) acc[k][m] = fma(cv[m], xv[k], acc[k][m]);
+            }
+        }
+    }
+    // fixed-order tree over the 8 warps: 4+4, 2+2, 1+1
+    T* red = reinterpret_cast<T*>(smraw);
+#pragma unroll 1
+    for (int h = 4; h >= 1; h >>= 1) {
+        __syncthreads();
+        if (w >= h && w < 2 * h) {
+            T* r = red + ((size_t)(w - h) * 32 + lane) * (4 * NPG);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int m = 0; m < NPG; ++m) r[k * NPG + m] = acc[k][m];
+        }
+        __syncthreads();
+        if (w < h) {
+            const T* r = red + ((size_t)w * 32 + lane) * (4 * NPG);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int m = 0; m < NPG; ++m) acc[k][m] += r[k * NPG + m];
+        }
+    }
+    if (w == 0) {
+#pragma unroll
+        for (int m = 0; m < NPG; ++m) {
+            const int j = pg * NPG + m;
+            if (j < np) {
+                const T sc = (T)(tab.gamma[poff + j] * dV);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int col = n0 + 4 * cg + k;
+                    if (col < ncolp) alpha[(long long)(poff + j) * ncolp + col] = sc * acc[k][m];
+                }
+            }
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    nl_scatter2_kernel(T* __restrict__ out, long long ld, int ncol, int ncolp, NLView tab,
+                       const int* __restrict__ imgs, const T* __restrict__ alpha, T scale) {
+    constexpr int NB = kNL2Cols, G = kNL2Pts;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int im = imgs[blockIdx.x];
+    const int n0 = blockIdx.y * NB;
+    const int a = tab.img_atom[im];
+    const int np = tab.atom_nproj[a];
+    const int poff = tab.atom_poff[a];
+    const int ndc = tab.img_ndc[im];
+    const int* gp = tab.gpos + tab.img_goff[im];
+    const T* ch = reinterpret_cast<const T*>(tab.chi) + tab.img_chi_off[im];
+    T* al = reinterpret_cast<T*>(smraw);  // [np][NB]
+    T* cs = al + (size_t)np * NB;         // [np][G]
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    for (int e = tid; e < np * NB; e += 256) {
+        const int j = e / NB, c = e % NB;
+        al[e] = (n0 + c < ncolp) ? alpha[(long long)(poff + j) * ncolp + n0 + c] : T(0);
+    }
+    for (int g0 = 0; g0 < ndc; g0 += G) {
+        __syncthreads();
+        for (int e = tid; e < np * G; e += 256) {
+            const int j = e / G, g = e % G;
+            cs[e] = (g0 + g < ndc) ? ch[(long long)j * ndc + g0 + g] : T(0);
+        }
+        __syncthreads();
+        T acc[2][8];
+#pragma unroll
+        for (int p = 0; p < 2; ++p)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[p][k] = T(0);
+        for (int j = 0; j < np; ++j) {
+            const T c0 = cs[j * G + lane], c1 = cs[j * G + lane + 32];
+            T av[8];
+            T t0[4], t1[4];
+            load_vec4(al + j * NB + 8 * w, t0);
+            load_vec4(al + j * NB + 8 * w + 4, t1);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                av[k] = t0[k];
+                av[k + 4] = t1[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                acc[0][k] = fma(c0, av[k], acc[0][k]);
+                acc[1][k] = fma(c1, av[k], acc[1][k]);
+            }
+        }
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            const int g = g0 + lane + 32 * p;
+            if (g < ndc) {
+                T* o = out + gp[g];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int col = n0 + 8 * w + k;
+                    if (col < ncol) {
+                        T* q = o + (long long)col * ld;
+                        *q = fma(scale, acc[p][k], *q);
+                    }
+                }
+            }
+        }
+    }
+}
+
 }  // namespace lynxb

@@ -31,6 +31,43 @@ NLView make_view(const NLDev& nl) {
     v.ent_loc = nl.ent_loc;
     return v;
 }
+template <typename T>
+constexpr bool kReal = std::is_same<T, float>::value || std::is_same<T, double>::value;
+
+int launch_status(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("%s launch failed: %s", what, cudaGetErrorString(e));
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+template <typename T, int NPG>
+int gather2(const NLDev& nl, const T* x, long long ld, int ncol, T* alpha, int ncolp, double dV, cudaStream_t st) {
+    const size_t smem = Gather2Geom<T, NPG>::smem_bytes;
+    auto kern = nl_gather2_kernel<T, NPG>;
+    if (smem > 48 * 1024) LYNX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid(nl.n_atom, (ncol + kNL2Cols - 1) / kNL2Cols);
+    kern<<<grid, 256, smem, st>>>(x, ld, ncol, ncolp, make_view<T>(nl), alpha, dV);
+    count_launch();
+    return launch_status("nonlocal gather");
+}
+
+// Register-tiled gather for real data: projector groups of NPG >= ceil(max_np / 2).
+template <typename T>
+int gather2_dispatch(const NLDev& nl, const T* x, long long ld, int ncol, T* alpha, int ncolp, double dV,
+                     cudaStream_t st) {
+    const int h = (nl.max_np + 1) / 2;
+    if (h <= 1) return gather2<T, 1>(nl, x, ld, ncol, alpha, ncolp, dV, st);
+    if (h <= 2) return gather2<T, 2>(nl, x, ld, ncol, alpha, ncolp, dV, st);
+    if (h <= 4) return gather2<T, 4>(nl, x, ld, ncol, alpha, ncolp, dV, st);
+    if (h <= 5) return gather2<T, 5>(nl, x, ld, ncol, alpha, ncolp, dV, st);
+    if (h <= 8) return gather2<T, 8>(nl, x, ld, ncol, alpha, ncolp, dV, st);
+    if (h <= 9) return gather2<T, 9>(nl, x, ld, ncol, alpha, ncolp, dV, st);
+    if (h <= 12) return gather2<T, 12>(nl, x, ld, ncol, alpha, ncolp, dV, st);
+    return gather2<T, 16>(nl, x, ld, ncol, alpha, ncolp, dV, st);
+}
 }  // namespace
 
 template <typename T>
@@ -40,6 +77,9 @@ int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alp
     constexpr int NB = 32;  // columns per CTA; 8 projector groups of 256 threads
     static_assert(kNLColBlock % 16 == 0 && NB % kNLColBlock == 0 || kNLColBlock % NB == 0, "column blocks");
     if (nl.n_atom == 0 || ncol <= 0) return LYNX_OK;
+    if constexpr (kReal<T>) {
+        if (nl.max_np <= 32) return gather2_dispatch<T>(nl, x, ld, ncol, alpha, ncolp, dV, st);
+    }
     const int pj = (nl.max_np + 7) / 8;
     if (pj > 4) {
         set_error("%d projectors per atom exceed the gather kernel's limit of 32", nl.max_np);
@@ -69,6 +109,21 @@ int launch_nl_scatter(const NLDev& nl, T* out, long long ld, int ncol, const T* 
                       cudaStream_t st) {
     constexpr int NB = 16;
     if (nl.n_pts == 0 || ncol <= 0) return LYNX_OK;
+    if constexpr (kReal<T>) {
+        if (nl.n_colors > 0 && nl.max_np <= 32) {
+            const size_t smem = sizeof(T) * 2 * (size_t)nl.max_np * kNL2Cols;
+            for (int k = 0; k < nl.n_colors; ++k) {
+                const int cnt = nl.color_off[k + 1] - nl.color_off[k];
+                if (cnt == 0) continue;
+                dim3 grid(cnt, (ncol + kNL2Cols - 1) / kNL2Cols);
+                nl_scatter2_kernel<T><<<grid, 256, smem, st>>>(out, ld, ncol, ncolp, make_view<T>(nl),
+                                                               nl.color_img + nl.color_off[k], alpha, (T)scale);
+                count_launch();
+                LYNX_TRY(launch_status("nonlocal scatter"));
+            }
+            return LYNX_OK;
+        }
+    }
     dim3 grid((nl.n_pts + 127) / 128, (ncol + NB - 1) / NB);
     nl_scatter_kernel<T, NB><<<grid, 128, 0, st>>>(out, ld, ncol, ncolp, make_view<T>(nl), alpha, scale);
     count_launch();
