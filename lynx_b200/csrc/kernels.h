@@ -32,7 +32,11 @@ inline int pipe_row_elems(int nx, size_t scalar_size) {
 template <typename T, typename S>
 int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out,
                      long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl, const T* phr,
-                     int* err, cudaStream_t st);
+                     int* err, cudaStream_t st, int shape = 0);
+// Number of launch shapes compiled for FD half-width R (shape indices 0 .. count-1; any shape
+// gives bitwise the same result, they differ in speed only).
+template <typename T>
+int pipe_shape_count(int R);
 
 // Rayleigh-Ritz Gram products Ms = dV Y^T Y (upper triangle), Hs = dV Y^T HY of FP32 blocks
 // (rows x n, column stride ld) on the tensor cores: exact int8-slice products, FP64 result,

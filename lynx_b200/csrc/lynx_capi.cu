@@ -14,6 +14,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -169,6 +170,8 @@ struct lynx_ctx {
     DevBuf gwork;           // slices, exponents and split partials of the tensor-core Gram
     DevBuf rwork;           // slices and exponents of the tensor-core rotation
     bool no_tc_gram = false;  // diagnostic switch: FP64 library products for the mixed path
+    bool autotune = true;     // time the compiled stencil launch shapes on first use per grid
+    std::map<std::array<long long, 6>, int> pipe_shape;  // chosen launch shape per (type, grid, columns)
     // nonlocal tables re-indexed for padded row layouts: nxp -> tables
     std::map<int, NLDev> nl_layouts;
     std::vector<DevBuf> nl_layout_bufs;
@@ -489,6 +492,62 @@ int check_errflag(lynx_ctx* c) {
 // One fused step: out = a*(H_loc x) + b*x + d*xold, plus the nonlocal part a*Vnl x.
 // Blocks use rows of length nxp (nxp == nx: the caller's unpadded layout); V uses the same rows.
 // 16-byte aligned layouts run the pipelined kernel, others the register-window kernel.
+// Launch-shape autotuner of the pipelined stencil.  The first launch for a given (type, grid,
+// columns) times every compiled shape on the actual arguments (one untimed launch each, to load
+// the module, then one timed launch) and keeps the fastest for the context; every shape writes
+// bitwise the same output, and the last timed launch leaves it in place.  The filter never
+// lets `out` alias `x` or `xold`, so repeating the launch is harmless.
+template <typename T, typename S>
+int pipe_launch_tuned(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out,
+                      long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl,
+                      const T* phr) {
+    const StencilGeom g = geom(c);
+    const int nsh = pipe_shape_count<T>(g.R);
+    const std::array<long long, 6> key = {(long long)sizeof(T), (long long)ScalarOf<T>::cplx, nxp, c->ny, c->nz,
+                                          ncol};
+    auto it = c->pipe_shape.find(key);
+    if (it != c->pipe_shape.end() || nsh <= 1 || !c->autotune) {
+        const int si = (it != c->pipe_shape.end()) ? it->second : 0;
+        return launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
+                                      c->errflag.as<int>(), c->stream, si);
+    }
+    cudaEvent_t e0, e1;
+    LYNX_CUDA_TRY(cudaEventCreate(&e0));
+    LYNX_CUDA_TRY(cudaEventCreate(&e1));
+    int best = 0;
+    float best_ms = 1e30f;
+    int rc = LYNX_OK;
+    for (int si = 0; si < nsh && rc == LYNX_OK; ++si) {
+        rc = launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
+                                    c->errflag.as<int>(), c->stream, si);
+        if (rc != LYNX_OK) break;
+        cudaEventRecord(e0, c->stream);
+        rc = launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
+                                    c->errflag.as<int>(), c->stream, si);
+        cudaEventRecord(e1, c->stream);
+        if (rc != LYNX_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            set_error("stencil autotuning failed: %s", cudaGetErrorString(cudaGetLastError()));
+            rc = LYNX_ERR_CUDA;
+            break;
+        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = si;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != LYNX_OK) return rc;
+    c->pipe_shape[key] = best;
+    if (best != nsh - 1)  // leave the chosen shape's (identical) output as the result of record
+        return launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
+                                      c->errflag.as<int>(), c->stream, best);
+    return LYNX_OK;
+}
+
 template <typename T>
 int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out, long long ldout,
               const typename Real<T>::type* V, int ncol, double a, double b, double d, bool use_k) {
@@ -511,8 +570,7 @@ int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, lo
     }
     if (pipe_ok) {
         if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
-        LYNX_TRY(launch_cheb_pipe<T, S>(geom(c), nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
-                                        c->errflag.as<int>(), c->stream));
+        LYNX_TRY(pipe_launch_tuned<T, S>(c, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr));
     } else {
         LYNX_TRY(launch_cheb_step<T, S>(geom(c), x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, c->stream));
     }

@@ -121,8 +121,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 // through column offsets wrapped once at start-up, and PHASED instantiations (Bloch phases,
 // Dirichlet zeros) multiply wrapped neighbours in registers.  Per stage two mbarriers:
 // full (copies landed, tx-counted) and empty (every consumer warp done reading).
-template <typename T, int R, int RX, int RY, bool XOLD, int NS, bool PHASED>
-__global__ void __launch_bounds__(kPipeMaxThreads, 1)
+template <typename T, int R, int RX, int RY, bool XOLD, int NS, bool PHASED, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1)
     cheb_pipe_kernel(const T* __restrict__ x, const T* __restrict__ xold, T* __restrict__ out,
                      const typename ScalarOf<T>::type* __restrict__ V, const PipeGeom G, const PipeCoef<T> C,
                      int* __restrict__ err) {
@@ -134,6 +134,7 @@ __global__ void __launch_bounds__(kPipeMaxThreads, 1)
     // x-neighbour vector loads: first element index rounded down to a multiple of RX
     constexpr int XOFF = (R % RX == 0) ? R : (R + RX - (R % RX));  // XOFF >= R, XOFF % RX == 0
     constexpr int NXV = (XOFF + R + RX + RX - 1) / RX;            // vectors covering x-XOFF .. x+RX-1+R
+    constexpr bool kPacked = std::is_same<T, float>::value && RX == 2;
 
     extern __shared__ __align__(128) unsigned char smpipe[];
     const int tid = threadIdx.x;
@@ -360,6 +361,85 @@ __global__ void __launch_bounds__(kPipeMaxThreads, 1)
         return true;
     };
 
+    // FP32 with RX = 2: the same sums in packed FP32x2 arithmetic (fma.rn.f32x2 / add / mul).
+    // Every output element sees exactly the scalar path's operations in the same order, so the
+    // results are bitwise identical; the instruction count of the z, y, V and x_old terms and of
+    // the even x offsets halves.
+    auto packed_plane = [&](auto Jc, int z, const T* tile, const T* xo_s, const S* v_s) {
+        if constexpr (kPacked) {
+            constexpr int J = decltype(Jc)::value;
+            float2 acc[RY];
+            const float2 dg = make_float2(C.diag, C.diag);
+#pragma unroll
+            for (int r = 0; r < RY; ++r) {
+                acc[r] = __fmul2_rn(dg, w[J + R][r]);
+#pragma unroll
+                for (int p = 1; p <= R; ++p)
+                    acc[r] = __ffma2_rn(make_float2(C.cz[p], C.cz[p]), __fadd2_rn(w[J + R + p][r], w[J + R - p][r]),
+                                        acc[r]);
+            }
+            {
+                const float* tcol = tile + (R + yl[0]) * nxp + xb;
+#pragma unroll
+                for (int q = -R; q < RY + R; ++q) {
+                    float2 v = *reinterpret_cast<const float2*>(tcol + q * nxp);
+                    if (PHASED) {
+                        if (ywrap_l & (1u << (q + R))) {
+                            v.x *= C.phl[1];
+                            v.y *= C.phl[1];
+                        } else if (ywrap_r & (1u << (q + R))) {
+                            v.x *= C.phr[1];
+                            v.y *= C.phr[1];
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < RY; ++r) {
+                        const int d = (q > r) ? q - r : r - q;
+                        if (d >= 1 && d <= R) acc[r] = __ffma2_rn(make_float2(C.cy[d], C.cy[d]), v, acc[r]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < RY; ++r) {
+                if (!own[r]) continue;
+                const float* trow = tile + (R + yl[r]) * nxp;
+                float2 P[NXV];
+#pragma unroll
+                for (int k = 0; k < NXV; ++k) {
+                    float2 t = *reinterpret_cast<const float2*>(trow + xcol[k]);
+                    if (PHASED) {
+                        if (xwrap & (1u << (2 * k))) {
+                            t.x *= C.phl[0];
+                            t.y *= C.phl[0];
+                        } else if (xwrap & (2u << (2 * k))) {
+                            t.x *= C.phr[0];
+                            t.y *= C.phr[0];
+                        }
+                    }
+                    P[k] = t;
+                }
+                constexpr int H = XOFF / 2;
+#pragma unroll
+                for (int p = 1; p <= R; ++p) {
+                    if (p % 2 == 0) {
+                        acc[r] = __ffma2_rn(make_float2(C.cx[p], C.cx[p]), __fadd2_rn(P[H + p / 2], P[H - p / 2]), acc[r]);
+                    } else {
+                        const float2 sl = __fadd2_rn(P[(XOFF - 1 + p) / 2], P[(XOFF - 1 - p) / 2]);
+                        const float2 sr = __fadd2_rn(P[(XOFF + 1 + p) / 2], P[(XOFF + 1 - p) / 2]);
+                        acc[r].x = fmaf(C.cx[p], sl.y, acc[r].x);
+                        acc[r].y = fmaf(C.cx[p], sr.x, acc[r].y);
+                    }
+                }
+                const int so = yl[r] * nxp + xb;
+                const float2 vv = *reinterpret_cast<const float2*>(v_s + so);
+                acc[r] = __ffma2_rn(__fmul2_rn(make_float2(C.a, C.a), vv), w[J + R][r], acc[r]);
+                if (XOLD) acc[r] = __ffma2_rn(make_float2(C.d, C.d), *reinterpret_cast<const float2*>(xo_s + so), acc[r]);
+                float* op = oc + (long long)z * G.plane + (long long)(y0 + yl[r]) * nxp + xb;
+                *reinterpret_cast<float2*>(op) = acc[r];
+            }
+        }
+    };
+
     // One plane with the window starting at slot J.
     auto plane_step = [&](auto Jc, int i) -> bool {
         constexpr int J = decltype(Jc)::value;
@@ -369,6 +449,9 @@ __global__ void __launch_bounds__(kPipeMaxThreads, 1)
         const T* tile = tile_of(st);
         const T* xo_s = XOLD ? xold_of(st) : nullptr;
         const S* v_s = veff_of(st);
+        if constexpr (kPacked) {
+            packed_plane(Jc, z, tile, xo_s, v_s);
+        } else {
         T acc[RY][RX];
         // centre, z neighbours
 #pragma unroll
@@ -463,6 +546,7 @@ __global__ void __launch_bounds__(kPipeMaxThreads, 1)
 #pragma unroll
             for (int u = 0; u < RX; ++u) opv[u] = acc[r][u];
             *reinterpret_cast<VT*>(op) = o;
+        }
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[st]);

@@ -12,41 +12,109 @@ namespace lynxb {
 
 namespace {
 
-template <typename T> struct PipeShape;
-// RX adjacent x points x RY rows per thread, launch-bound thread count.
-template <> struct PipeShape<float> { static constexpr int RX = 2, RY = 4; };
-template <> struct PipeShape<double> { static constexpr int RX = 2, RY = 2; };
-template <> struct PipeShape<float2> { static constexpr int RX = 1, RY = 4; };
-template <> struct PipeShape<double2> { static constexpr int RX = 1, RY = 2; };
+// Launch shapes: RX adjacent x points x RY rows per thread, launch-bound thread count (which
+// sets the register budget).  Shape 0 is the default; for the common FD half-width kTunedR the
+// other shapes are compiled too and chosen per grid by the caller's autotuner (they trade
+// registers per thread, i.e. window rows, against resident warps).
+template <typename T, int I> struct PipeShapeAt;
+template <> struct PipeShapeAt<float, 0> { static constexpr int RX = 2, RY = 4, MAXT = 352; };
+template <> struct PipeShapeAt<float, 1> { static constexpr int RX = 2, RY = 3, MAXT = 512; };
+template <> struct PipeShapeAt<float, 2> { static constexpr int RX = 2, RY = 2, MAXT = 512; };
+template <> struct PipeShapeAt<float, 3> { static constexpr int RX = 2, RY = 3, MAXT = 448; };
+template <> struct PipeShapeAt<double, 0> { static constexpr int RX = 2, RY = 2, MAXT = 352; };
+template <> struct PipeShapeAt<double, 1> { static constexpr int RX = 2, RY = 1, MAXT = 512; };
+template <> struct PipeShapeAt<double, 2> { static constexpr int RX = 2, RY = 1, MAXT = 640; };
+template <> struct PipeShapeAt<double, 3> { static constexpr int RX = 2, RY = 2, MAXT = 384; };
+template <> struct PipeShapeAt<float2, 0> { static constexpr int RX = 1, RY = 4, MAXT = 352; };
+template <> struct PipeShapeAt<double2, 0> { static constexpr int RX = 1, RY = 2, MAXT = 352; };
+template <typename T> struct NumShapes { static constexpr int value = 1; };
+template <> struct NumShapes<float> { static constexpr int value = 4; };
+template <> struct NumShapes<double> { static constexpr int value = 4; };
+constexpr int kTunedR = 6;  // FD order 12
 
-template <typename T, int R, bool XOLD, bool PH>
+struct ShapeRT {
+    int RX, RY, MAXT;
+};
+template <typename T, int I>
+ShapeRT shape_i() {
+    using P = PipeShapeAt<T, I>;
+    return {P::RX, P::RY, P::MAXT};
+}
+template <typename T>
+ShapeRT shape_rt(int si) {
+    if constexpr (NumShapes<T>::value > 1) {
+        switch (si) {
+            case 1: return shape_i<T, 1>();
+            case 2: return shape_i<T, 2>();
+            case 3: return shape_i<T, 3>();
+            default: break;
+        }
+    }
+    return shape_i<T, 0>();
+}
+
+template <typename T, int R, bool XOLD, bool PH, int SI>
 void launch_pipe_ph(int ns, dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x, const T* xo, T* out,
                     const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C, int* err) {
-    constexpr int RX = PipeShape<T>::RX, RY = PipeShape<T>::RY;
-    auto kern = ns >= 5 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 5, PH>
-               : (ns == 4 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 4, PH> : cheb_pipe_kernel<T, R, RX, RY, XOLD, 3, PH>);
+    using P = PipeShapeAt<T, SI>;
+    constexpr int RX = P::RX, RY = P::RY, MT = P::MAXT;
+    auto kern = ns >= 5 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 5, PH, MT>
+               : (ns == 4 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 4, PH, MT>
+                          : cheb_pipe_kernel<T, R, RX, RY, XOLD, 3, PH, MT>);
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     kern<<<grid, nthr, smem, st>>>(x, xo, out, V, G, C, err);
 }
 
 // Real data with periodic boundaries needs no phase on wrapped neighbours; complex data and
-// Dirichlet boundaries use the PHASED instantiation.
+// Dirichlet boundaries use the PHASED instantiation (default shape only).
 template <typename T, int R, bool XOLD>
-void launch_pipe(int ns, bool phased, dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x, const T* xo,
-                 T* out, const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C, int* err) {
-    if (ScalarOf<T>::cplx || phased) launch_pipe_ph<T, R, XOLD, true>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err);
-    else launch_pipe_ph<T, R, XOLD, false>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err);
+void launch_pipe(int si, int ns, bool phased, dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x,
+                 const T* xo, T* out, const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C,
+                 int* err) {
+    if (ScalarOf<T>::cplx || phased) {
+        launch_pipe_ph<T, R, XOLD, true, 0>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err);
+        return;
+    }
+    if constexpr (R == kTunedR && NumShapes<T>::value > 1) {
+        switch (si) {
+            case 1: launch_pipe_ph<T, R, XOLD, false, 1>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err); return;
+            case 2: launch_pipe_ph<T, R, XOLD, false, 2>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err); return;
+            case 3: launch_pipe_ph<T, R, XOLD, false, 3>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err); return;
+            default: break;
+        }
+    }
+    launch_pipe_ph<T, R, XOLD, false, 0>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err);
+}
+
+template <typename T>
+bool phases_trivial(const T* phl, const T* phr) {
+    using S = typename ScalarOf<T>::type;
+    for (int k = 0; k < 3; ++k) {
+        const S* l = reinterpret_cast<const S*>(&phl[k]);
+        const S* r = reinterpret_cast<const S*>(&phr[k]);
+        for (int c = 0; c < (int)(sizeof(T) / sizeof(S)); ++c)
+            if (l[c] != (c == 0 ? S(1) : S(0)) || r[c] != (c == 0 ? S(1) : S(0))) return false;
+    }
+    return true;
 }
 
 }  // namespace
 
+template <typename T>
+int pipe_shape_count(int R) {
+    return (R == kTunedR) ? NumShapes<T>::value : 1;
+}
+
 template <typename T, typename S>
 int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out,
                      long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl, const T* phr,
-                     int* err, cudaStream_t st) {
+                     int* err, cudaStream_t st, int shape) {
     static_assert(std::is_same<S, typename ScalarOf<T>::type>::value, "scalar type mismatch");
-    constexpr int RX = PipeShape<T>::RX, RY = PipeShape<T>::RY;
     const int R = g.R;
+    const bool phased = ScalarOf<T>::cplx || !phases_trivial(phl, phr);
+    const int si = (shape > 0 && shape < pipe_shape_count<T>(R) && !phased) ? shape : 0;
+    const ShapeRT sh = shape_rt<T>(si);
+    const int RX = sh.RX, RY = sh.RY, MT = sh.MAXT;
     if (R < 1 || R > 8) {
         set_error("FD half-width %d outside the supported range 1..8", R);
         return LYNX_ERR_UNSUPPORTED;
@@ -66,13 +134,14 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
     }
     if (ncol <= 0) return LYNX_OK;
     const int P2 = g.nx / RX;
-    if (P2 > kPipeMaxThreads - 32) {
+    if (P2 > MT - 32) {
         set_error("nx = %d too large for the pipelined stencil", g.nx);
         return LYNX_ERR_UNSUPPORTED;
     }
-    // One CTA per SM: ~288 consumer threads (whole x-rows per thread row), bands balanced over ny.
-    int TYT = std::max(1, (288 + P2 / 2) / P2);
-    TYT = std::min(TYT, (kPipeMaxThreads - 32) / P2);
+    // One CTA per SM: about MT - 64 consumer threads (whole x-rows per thread row), bands
+    // balanced over ny.
+    int TYT = std::max(1, (MT - 64 + P2 / 2) / P2);
+    TYT = std::min(TYT, (MT - 32) / P2);
     TYT = std::min(TYT, (g.ny + RY - 1) / RY);
     {
         const int nb = (g.ny + TYT * RY - 1) / (TYT * RY);
@@ -131,18 +200,11 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
         C.phl[k] = phl[k];
         C.phr[k] = phr[k];
     }
-    bool phased = false;
-    for (int k = 0; k < 3; ++k) {
-        const S* l = reinterpret_cast<const S*>(&phl[k]);
-        const S* r = reinterpret_cast<const S*>(&phr[k]);
-        for (int c = 0; c < (int)(sizeof(T) / sizeof(S)); ++c)
-            if (l[c] != (c == 0 ? S(1) : S(0)) || r[c] != (c == 0 ? S(1) : S(0))) phased = true;
-    }
     dim3 grid(nbands, ncol, nzch);
 #define LYNX_PIPE_CASE(RR)                                                                       \
     case RR:                                                                                     \
-        if (xo) launch_pipe<T, RR, true>(ns, phased, grid, nthr, smem, st, x, xold, out, V, G, C, err);       \
-        else launch_pipe<T, RR, false>(ns, phased, grid, nthr, smem, st, x, xold, out, V, G, C, err);         \
+        if (xo) launch_pipe<T, RR, true>(si, ns, phased, grid, nthr, smem, st, x, xold, out, V, G, C, err);   \
+        else launch_pipe<T, RR, false>(si, ns, phased, grid, nthr, smem, st, x, xold, out, V, G, C, err);     \
         break;
     switch (R) {
         LYNX_PIPE_CASE(1)
@@ -167,17 +229,21 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
 #if LYNX_STENCIL_TYPES == 0
 template int launch_cheb_pipe<double, double>(const StencilGeom&, int, const double*, long long, const double*,
                                               long long, double*, long long, const double*, int, double, double,
-                                              double, const double*, const double*, int*, cudaStream_t);
+                                              double, const double*, const double*, int*, cudaStream_t, int);
 template int launch_cheb_pipe<float, float>(const StencilGeom&, int, const float*, long long, const float*,
                                             long long, float*, long long, const float*, int, double, double, double,
-                                            const float*, const float*, int*, cudaStream_t);
+                                            const float*, const float*, int*, cudaStream_t, int);
+template int pipe_shape_count<double>(int);
+template int pipe_shape_count<float>(int);
 #else
 template int launch_cheb_pipe<double2, double>(const StencilGeom&, int, const double2*, long long, const double2*,
                                                long long, double2*, long long, const double*, int, double, double,
-                                               double, const double2*, const double2*, int*, cudaStream_t);
+                                               double, const double2*, const double2*, int*, cudaStream_t, int);
 template int launch_cheb_pipe<float2, float>(const StencilGeom&, int, const float2*, long long, const float2*,
                                              long long, float2*, long long, const float*, int, double, double,
-                                             double, const float2*, const float2*, int*, cudaStream_t);
+                                             double, const float2*, const float2*, int*, cudaStream_t, int);
+template int pipe_shape_count<double2>(int);
+template int pipe_shape_count<float2>(int);
 #endif
 
 }  // namespace lynxb
