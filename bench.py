@@ -46,6 +46,21 @@ CONFIGS = {
 }
 
 
+def replica_seed(rank: int) -> int:
+    """Seed of a replica's start orbitals: with --gpus N every rank solves its own problem."""
+    return 1234 + rank
+
+
+def max_over_ranks(seconds: float, world: int, device) -> float:
+    """The job's time is the slowest replica's: an all-reduce MAX over the ranks (no-op at N=1)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([seconds], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -249,7 +264,7 @@ def main():
     es = solver.EigenSolver(ctx, args.precision)
     lo, hi = es.lanczos_bounds(Vd)
     lc, emin = 0.5 * (lo + hi), lo
-    gen = torch.Generator(device="cuda").manual_seed(1234 + rank)
+    gen = torch.Generator(device="cuda").manual_seed(replica_seed(rank))
     psi = (torch.rand((nst, ctx.nd), generator=gen, device="cuda", dtype=torch.float64) - 0.5).contiguous()
 
     def one_pass(precision):
@@ -297,10 +312,7 @@ def main():
     with ClockSampler(local) as clk:
         t_main = timed(args.precision, args.steps)
     launches = int(lib.lynx_launch_count(1))
-    t = torch.tensor([t_main], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    t_main = float(t.item())
+    t_main = max_over_ranks(t_main, world, "cuda")
 
     # Roofline of the dominant kernel: the fused Chebyshev step, timed alone with CUDA events.
     import ctypes
