@@ -101,6 +101,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
         : "r"(taddr));
 }
 
+// Exact powers of two, built from the IEEE-754 exponent field (the argument is clamped to the
+// normal range; data whose scale leaves it would lose its slices to underflow, not fault).
+__device__ __forceinline__ float pow2f(int k) {
+    k = max(-126, min(127, k));
+    return __int_as_float((127 + k) << 23);
+}
+__device__ __forceinline__ double pow2d(int k) {
+    k = max(-1022, min(1023, k));
+    return __longlong_as_double((long long)(1023 + k) << 52);
+}
+
 struct GramArgs {
     int ksteps;     // K steps of BK over the whole (padded) K range
     int kper;       // K steps per split
@@ -227,7 +238,7 @@ __global__ void __launch_bounds__(128, 1)
         if (ok) {
             const int* eA = g.eY + (long long)split * g.npad;
             const int* eB = (prod ? g.eH : g.eY) + (long long)split * g.npad;
-            const int ea = eA[row];
+            const double sa = pow2d(eA[row]);
             const uint32_t lb = (uint32_t)(warp * 32) << 16;
 #pragma unroll 1
             for (int c0 = 0; c0 < BN; c0 += 16) {
@@ -242,7 +253,7 @@ __global__ void __launch_bounds__(128, 1)
                     // exact: the three terms span bits 2^17 .. 2^-28 (< 53 bits)
                     const double x = (double)(int)r2[t] * 0x1p-14 + (double)(int)r3[t] * 0x1p-21 +
                                      (double)(int)r4[t] * 0x1p-28;
-                    v[t] = ldexp(x, ea + eB[n0 + c0 + t]);
+                    v[t] = x * sa * pow2d(eB[n0 + c0 + t]);  // exact: powers of two
                 }
                 double2* dst = reinterpret_cast<double2*>(wrow + c0);
 #pragma unroll
@@ -261,20 +272,41 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
-// One K chunk of one column of an FP32 block -> exponent e and three int8 slices (column
-// stride ldk; rows rows..ldk-1 of the padded K range written as zero).
-__global__ void __launch_bounds__(256)
-    slice_i8_kernel(int8_t* __restrict__ s1, int8_t* __restrict__ s2, int8_t* __restrict__ s3, long long ldk,
-                    int* __restrict__ eexp, int npad, const float* __restrict__ y, long long ldy, long long rows,
-                    long long chunk) {
+// t = y 2^(7-e), |t| < 64 -> three int8 slices, each rounded to nearest (all steps exact).
+__device__ __forceinline__ void slice3(float t, int8_t& a, int8_t& b, int8_t& c) {
+    const float fa = rintf(t);
+    t = (t - fa) * 128.0f;
+    const float fb = rintf(t);
+    t = (t - fb) * 128.0f;
+    const float fc = rintf(t);
+    a = (int8_t)(int)fa;
+    b = (int8_t)(int)fb;
+    c = (int8_t)(int)fc;
+}
+
+struct SliceArgs {
+    int8_t* s[6];     // Y slices 1..3, HY slices 1..3: [n][ldk]
+    int* e[2];        // exponents of Y, HY: [nsplit][npad]
+    const float* y[2];
+    long long ldy, rows, ldk, chunk;
+    int npad;
+};
+
+// One K chunk of one column of an FP32 block (blockIdx.z: Y or HY) -> exponent e and three int8
+// slices (rows rows..ldk-1 of the padded K range written as zero).  ldy, rows, chunk and ldk
+// are multiples of 4, so the chunk is read as float4 and written as char4.
+__global__ void __launch_bounds__(256) slice_i8_kernel(const SliceArgs a) {
     __shared__ float red[8];
-    const int split = blockIdx.x, j = blockIdx.y;
-    const long long r0 = (long long)split * chunk;
-    const long long r1 = min(r0 + chunk, ldk);
-    const long long rend = min(r1, rows);
-    const float* col = y + (long long)j * ldy;
+    const int split = blockIdx.x, j = blockIdx.y, op = blockIdx.z;
+    const long long r0 = (long long)split * a.chunk;
+    const long long r1 = min(r0 + a.chunk, a.ldk);
+    const long long rend = min(r1, a.rows);
+    const float* col = a.y[op] + (long long)j * a.ldy;
     float m = 0.0f;
-    for (long long r = r0 + threadIdx.x; r < rend; r += blockDim.x) m = fmaxf(m, fabsf(col[r]));
+    for (long long r = r0 + 4 * threadIdx.x; r < rend; r += 4 * blockDim.x) {
+        const float4 v = *reinterpret_cast<const float4*>(col + r);
+        m = fmaxf(fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y))), fmaxf(fabsf(v.z), fabsf(v.w)));
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
@@ -285,20 +317,22 @@ __global__ void __launch_bounds__(256)
     int E = 0;
     if (m > 0.0f) frexpf(m, &E);  // m = f 2^E, f in [1/2, 1)
     const int e = (m > 0.0f) ? E + 1 : 0;  // |y| 2^-e < 1/2
-    if (threadIdx.x == 0) eexp[(long long)split * npad + j] = e;
-    int8_t* o1 = s1 + (long long)j * ldk;
-    int8_t* o2 = s2 + (long long)j * ldk;
-    int8_t* o3 = s3 + (long long)j * ldk;
-    for (long long r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-        float t = (r < rows) ? ldexpf(col[r], 7 - e) : 0.0f;  // exact: power-of-two scaling
-        const float a = rintf(t);                               // |t| < 64
-        t = (t - a) * 128.0f;                                   // exact, |t| <= 64
-        const float b = rintf(t);
-        t = (t - b) * 128.0f;
-        const float c = rintf(t);
-        o1[r] = (int8_t)(int)a;
-        o2[r] = (int8_t)(int)b;
-        o3[r] = (int8_t)(int)c;
+    if (threadIdx.x == 0) a.e[op][(long long)split * a.npad + j] = e;
+    const float sc = pow2f(7 - e);
+    int8_t* o1 = a.s[3 * op] + (long long)j * a.ldk;
+    int8_t* o2 = a.s[3 * op + 1] + (long long)j * a.ldk;
+    int8_t* o3 = a.s[3 * op + 2] + (long long)j * a.ldk;
+    for (long long r = r0 + 4 * threadIdx.x; r < r1; r += 4 * blockDim.x) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (r < a.rows) v = *reinterpret_cast<const float4*>(col + r);
+        char4 c1, c2, c3;
+        slice3(v.x * sc, reinterpret_cast<int8_t&>(c1.x), reinterpret_cast<int8_t&>(c2.x), reinterpret_cast<int8_t&>(c3.x));
+        slice3(v.y * sc, reinterpret_cast<int8_t&>(c1.y), reinterpret_cast<int8_t&>(c2.y), reinterpret_cast<int8_t&>(c3.y));
+        slice3(v.z * sc, reinterpret_cast<int8_t&>(c1.z), reinterpret_cast<int8_t&>(c2.z), reinterpret_cast<int8_t&>(c3.z));
+        slice3(v.w * sc, reinterpret_cast<int8_t&>(c1.w), reinterpret_cast<int8_t&>(c2.w), reinterpret_cast<int8_t&>(c3.w));
+        *reinterpret_cast<char4*>(o1 + r) = c1;
+        *reinterpret_cast<char4*>(o2 + r) = c2;
+        *reinterpret_cast<char4*>(o3 + r) = c3;
     }
 }
 
@@ -417,8 +451,8 @@ struct RotArgs {
     int ntn;          // output column tiles
     long long rows;   // rows of the padded Y block
     int nx, nxp;      // row padding: r = x + nxp * rest, x < nx valid
-    const int* erow;  // [rows] row exponents
-    const int* fcol;  // [N] column exponents
+    const int* erow;     // [rows] row exponents
+    const double* fpow;  // [N] column scales 2^f
     double* psi;      // output, column stride ldp, unpadded rows
     long long ldp;
     int* err;
@@ -516,11 +550,11 @@ __global__ void __launch_bounds__(128, 1)
     if (ok) {
         const long long row = (long long)m0 + warp * 32 + lane;
         long long ridx = -1;
-        int er = 0;
+        double rs = 1.0;
         if (row < g.rows) {
             const long long xr = row % g.nxp, rest = row / g.nxp;
             if (xr < g.nx) ridx = xr + (long long)g.nx * rest;
-            er = g.erow[row];
+            rs = pow2d(g.erow[row]);
         }
         const uint32_t lb = (uint32_t)(warp * 32) << 16;
 #pragma unroll 1
@@ -537,7 +571,7 @@ __global__ void __launch_bounds__(128, 1)
                     if (j < g.N) {
                         const double x = (double)(int)r2[t] * 0x1p-14 + (double)(int)r3[t] * 0x1p-21 +
                                          (double)(int)r4[t] * 0x1p-28;
-                        g.psi[(long long)j * g.ldp + ridx] = ldexp(x, er + g.fcol[j]);
+                        g.psi[(long long)j * g.ldp + ridx] = x * rs * g.fpow[j];  // exact: powers of two
                     }
                 }
             }
@@ -574,7 +608,7 @@ __global__ void __launch_bounds__(256)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = w; i < N; i += 8) {
         const long long r = r0 + lane;
-        tsm[i * 33 + lane] = (r < rows) ? ldexpf(y[(long long)i * ldy + r], -dcol[i]) : 0.0f;
+        tsm[i * 33 + lane] = (r < rows) ? y[(long long)i * ldy + r] * pow2f(-dcol[i]) : 0.0f;
     }
     __syncthreads();
     for (int rr = w; rr < 32; rr += 8) {
@@ -592,6 +626,7 @@ __global__ void __launch_bounds__(256)
         if (r >= rows) continue;
         const int e = es[rr];
         if (lane == 0) erow[r] = e;
+        const float sc = pow2f(7 - e);
         for (int i0 = 4 * lane; i0 < ldk; i0 += 128) {
             char4 o1, o2, o3;
             int8_t* p1 = reinterpret_cast<int8_t*>(&o1);
@@ -600,15 +635,7 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const int i = i0 + q;
-                float t = (i < N) ? ldexpf(tsm[i * 33 + rr], 7 - e) : 0.0f;
-                const float a = rintf(t);
-                t = (t - a) * 128.0f;
-                const float b = rintf(t);
-                t = (t - b) * 128.0f;
-                const float c = rintf(t);
-                p1[q] = (int8_t)(int)a;
-                p2[q] = (int8_t)(int)b;
-                p3[q] = (int8_t)(int)c;
+                slice3((i < N) ? tsm[i * 33 + rr] * sc : 0.0f, p1[q], p2[q], p3[q]);
             }
             *reinterpret_cast<char4*>(a1 + r * ldk + i0) = o1;
             *reinterpret_cast<char4*>(a2 + r * ldk + i0) = o2;
@@ -620,7 +647,7 @@ __global__ void __launch_bounds__(256)
 // Columns of 2^d W (FP64, column-major N x N) -> exponent f_j and three int8 slices b_q[j][i].
 __global__ void __launch_bounds__(128)
     slice_w_kernel(int8_t* __restrict__ b1, int8_t* __restrict__ b2, int8_t* __restrict__ b3, long long ldk,
-                   int* __restrict__ fcol, const double* __restrict__ W, int N, const int* __restrict__ dcol) {
+                   double* __restrict__ fpow, const double* __restrict__ W, int N, const int* __restrict__ dcol) {
     __shared__ double red[4];
     const int j = blockIdx.x;
     const double* col = W + (long long)j * N;
@@ -634,7 +661,7 @@ __global__ void __launch_bounds__(128)
     int E = 0;
     if (m > 0.0) frexp(m, &E);
     const int f = (m > 0.0) ? E + 1 : 0;
-    if (threadIdx.x == 0) fcol[j] = f;
+    if (threadIdx.x == 0) fpow[j] = pow2d(f);
     for (int i = threadIdx.x; i < ldk; i += blockDim.x) {
         double t = (i < N) ? ldexp(col[i], dcol[i] + 7 - f) : 0.0;
         const double a = rint(t);
@@ -657,6 +684,10 @@ int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows
         set_error("Gram workspace too small or misaligned");
         return LYNX_ERR_BAD_ARG;
     }
+    if ((ld % 4) || (rows % 4) || (reinterpret_cast<uintptr_t>(Y) & 15) || (reinterpret_cast<uintptr_t>(HY) & 15)) {
+        set_error("tensor-core Gram needs 16-byte aligned columns and a row count divisible by 4");
+        return LYNX_ERR_BAD_ARG;
+    }
     unsigned char* w = static_cast<unsigned char*>(work);
     int8_t* sl[6];
     for (int q = 0; q < 6; ++q) sl[q] = reinterpret_cast<int8_t*>(w + q * p.slice_bytes);
@@ -665,10 +696,20 @@ int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows
     double* ws = reinterpret_cast<double*>(w + 6 * p.slice_bytes + 2 * p.exp_bytes);
     const long long chunk = (long long)p.kper * BK;
     {
-        dim3 grid(p.nsplit, n);
-        slice_i8_kernel<<<grid, 256, 0, st>>>(sl[0], sl[1], sl[2], p.ldk, eY, p.npad, Y, ld, rows, chunk);
-        slice_i8_kernel<<<grid, 256, 0, st>>>(sl[3], sl[4], sl[5], p.ldk, eH, p.npad, HY, ld, rows, chunk);
-        count_launch(2);
+        SliceArgs sa;
+        for (int q = 0; q < 6; ++q) sa.s[q] = sl[q];
+        sa.e[0] = eY;
+        sa.e[1] = eH;
+        sa.y[0] = Y;
+        sa.y[1] = HY;
+        sa.ldy = ld;
+        sa.rows = rows;
+        sa.ldk = p.ldk;
+        sa.chunk = chunk;
+        sa.npad = p.npad;
+        dim3 grid(p.nsplit, n, 2);
+        slice_i8_kernel<<<grid, 256, 0, st>>>(sa);
+        count_launch();
     }
     CUtensorMap m[6];
     for (int q = 0; q < 6; ++q) LYNX_TRY(make_map(&m[q], sl[q], p.ldk, n));
@@ -706,7 +747,7 @@ RotPlan rot_plan(long long rows, int n) {
     p.a_bytes = align256((size_t)rows * p.ldk);
     p.b_bytes = align256((size_t)n * p.ldk);
     p.erow_bytes = align256((size_t)rows * sizeof(int));
-    p.col_bytes = align256((size_t)n * sizeof(int));
+    p.col_bytes = align256((size_t)n * sizeof(double));
     p.work_bytes = 3 * p.a_bytes + 3 * p.b_bytes + p.erow_bytes + 2 * p.col_bytes;
     p.smem_rows = (size_t)n * 33 * sizeof(float);
     return p;
@@ -736,12 +777,12 @@ int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp
     for (int q = 0; q < 3; ++q) b[q] = reinterpret_cast<int8_t*>(w + 3 * p.a_bytes + q * p.b_bytes);
     int* erow = reinterpret_cast<int*>(w + 3 * p.a_bytes + 3 * p.b_bytes);
     int* dcol = reinterpret_cast<int*>(w + 3 * p.a_bytes + 3 * p.b_bytes + p.erow_bytes);
-    int* fcol = dcol + p.col_bytes / sizeof(int);
+    double* fpow = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(dcol) + p.col_bytes);
     LYNX_CUDA_TRY(cudaFuncSetAttribute(slice_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)p.smem_rows));
     slice_rows_kernel<<<(unsigned)((rows + 31) / 32), 256, p.smem_rows, st>>>(a[0], a[1], a[2], p.ldk, erow, Y, ldy,
                                                                                rows, n, dcol);
-    slice_w_kernel<<<n, 128, 0, st>>>(b[0], b[1], b[2], p.ldk, fcol, W, n, dcol);
+    slice_w_kernel<<<n, 128, 0, st>>>(b[0], b[1], b[2], p.ldk, fpow, W, n, dcol);
     count_launch(2);
     CUtensorMap m[6];
     for (int q = 0; q < 3; ++q) LYNX_TRY(make_map_k(&m[q], a[q], p.ldk, n, rows));
@@ -754,7 +795,7 @@ int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp
     g.nx = nx;
     g.nxp = nxp;
     g.erow = erow;
-    g.fcol = fcol;
+    g.fpow = fpow;
     g.psi = psi;
     g.ldp = ldp;
     g.err = err;
