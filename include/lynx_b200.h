@@ -191,6 +191,17 @@ LYNX_API int lynx_time_filter_step(lynx_ctx* ctx, const double* veff, int ncol, 
  * one-time set-up and should come before any stream capture.  Real (Gamma-point) FP64 only. */
 LYNX_API int lynx_nonlocal_apply_noalloc(lynx_ctx* ctx, const double* psi, double* hpsi, int ncol, int ld);
 
+/* Execution options of a context (no counterpart in the reference; both settings compute the
+ * same results, bitwise):
+ *   LYNX_OPT_AUTOTUNE:       1 (default) times the compiled stencil launch shapes on the first
+ *                            launch for each grid and column count and keeps the fastest; 0 uses
+ *                            the default shape.
+ *   LYNX_OPT_FUSE_NONLOCAL:  1 adds the nonlocal term inside the stencil kernel when the
+ *                            projector spheres are disjoint (compact per-point copies between
+ *                            steps); 0 (default) uses the separate gather and scatter kernels. */
+enum { LYNX_OPT_AUTOTUNE = 1, LYNX_OPT_FUSE_NONLOCAL = 2 };
+LYNX_API int lynx_set_option(lynx_ctx* ctx, int option, int value);
+
 /* Number of kernel launches this library issued since the last reset (diagnostic counter). */
 LYNX_API long long lynx_launch_count(int reset);
 

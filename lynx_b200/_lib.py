@@ -13,6 +13,8 @@ LIB_PATH = os.path.join(_HERE, "liblynxb200.so")
 
 LYNX_OK = 0
 LYNX_ERR_BAD_ARG = 1
+OPT_AUTOTUNE = 1
+OPT_FUSE_NONLOCAL = 2
 LYNX_ERR_CUDA = 2
 LYNX_ERR_OOM = 3
 LYNX_ERR_CHOL_FAIL = 4
@@ -61,6 +63,7 @@ _SIGNATURES = {
     "lynx_hamiltonian_apply_kpt": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double]),
     "lynx_nonlocal_apply": (_c_int, [_p, _p, _p, _c_int, _c_int]),
     "lynx_nonlocal_apply_noalloc": (_c_int, [_p, _p, _p, _c_int, _c_int]),
+    "lynx_set_option": (_c_int, [_p, _c_int, _c_int]),
     "lynx_nonlocal_apply_kpt": (_c_int, [_p, _p, _p, _c_int, _c_int]),
     "lynx_chebyshev_filter": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _c_int]),
     "lynx_chebyshev_filter_kpt": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _c_int]),

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 namespace lynxb {
 
@@ -27,12 +28,25 @@ inline int pipe_row_elems(int nx, size_t scalar_size) {
     return ((nx + q - 1) / q) * q;
 }
 
+// Fused nonlocal term for the pipelined stencil: out += a * W[ptmap[point]] at sphere points
+// (W: compact (chi alpha) values, column stride ldw; ptmap row pitch mp; rowstart and its host
+// copy: first compact point number of every grid row (z * ny + y), nz * ny + 1 entries).
+struct PipeNLHost {
+    const void* W;
+    long long ldw;
+    const int* ptmap;
+    int mp;
+    const int* rowstart;
+    const std::vector<int>* rowstart_host;
+    void* xs_out;  // optional compact copy of out at the sphere points (column stride ldw)
+};
+
 // Pipelined stencil on 16-byte aligned, row-padded (nxp) blocks; V padded the same way.
 // err: device int set to 1 if a bounded shared-memory wait gives up.
 template <typename T, typename S>
 int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out,
                      long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl, const T* phr,
-                     int* err, cudaStream_t st, int shape = 0);
+                     int* err, cudaStream_t st, int shape = 0, const struct PipeNLHost* nlh = nullptr);
 // Number of launch shapes compiled for FD half-width R (shape indices 0 .. count-1; any shape
 // gives bitwise the same result, they differ in speed only).
 template <typename T>
@@ -83,6 +97,13 @@ struct NLDev {
     int n_colors = 0;
     int color_off[kNLMaxColors + 1] = {};
     int* color_img = nullptr;
+    // Compact per-point form (only when no grid point lies in two spheres): the distinct
+    // points numbered in grid order, ent_pt[entry] = point number of every (image, point) entry.
+    bool compact = false;
+    int* ent_pt = nullptr;
+    int2* pt_meta = nullptr;     // [n_pts] (first projector row, projector count) of the point's atom
+    double* chi_pt64 = nullptr;  // [max_np][n_pts] projector values in point order
+    float* chi_pt32 = nullptr;
     int* atom_img_ptr = nullptr;
     int* atom_img_list = nullptr;
     int* atom_nproj = nullptr;
@@ -111,5 +132,8 @@ int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alp
 template <typename T, typename S>
 int launch_nl_scatter(const NLDev& nl, T* out, long long ld, int ncol, const T* alpha, int ncolp, S scale,
                       cudaStream_t st);
+// W[col * ldw + point] = (chi alpha)(point, col) on the compact point numbering (nl.compact).
+template <typename T>
+int launch_nl_expand(const NLDev& nl, T* W, long long ldw, int ncol, const T* alpha, int ncolp, cudaStream_t st);
 
 }  // namespace lynxb

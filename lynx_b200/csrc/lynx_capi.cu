@@ -171,7 +171,16 @@ struct lynx_ctx {
     DevBuf rwork;           // slices and exponents of the tensor-core rotation
     bool no_tc_gram = false;  // diagnostic switch: FP64 library products for the mixed path
     bool autotune = true;     // time the compiled stencil launch shapes on first use per grid
-    std::map<std::array<long long, 6>, int> pipe_shape;  // chosen launch shape per (type, grid, columns)
+    std::map<std::array<long long, 7>, int> pipe_shape;  // chosen launch shape per (type, grid, columns, fused)
+    bool fuse_nl = false;     // add the nonlocal term inside the stencil when the spheres are disjoint
+    struct NLMap {
+        DevBuf ptmap, rowstart;
+        std::vector<int> rowstart_h;
+        int mp = 0;
+    };
+    std::map<int, NLMap> nl_maps;  // per padded row length: compact point map of the sphere points
+    DevBuf nlW;                    // compact (chi alpha) values, columns of ldw
+    DevBuf xsbuf[2];               // compact sphere-point copies of consecutive filter blocks
     // nonlocal tables re-indexed for padded row layouts: nxp -> tables
     std::map<int, NLDev> nl_layouts;
     std::vector<DevBuf> nl_layout_bufs;
@@ -462,6 +471,37 @@ int nl_for(lynx_ctx* c, int nxp, const NLDev** out) {
     return LYNX_OK;
 }
 
+// Compact point map of the sphere points for rows of length nxp (row pitch mp = nxp rounded up
+// to 4): ptmap[(z * ny + y) * mp + x] = compact number of grid point (x, y, z) or -1, and
+// rowstart[z * ny + y] = compact number of the first sphere point at or after that row.
+int nl_map_for(lynx_ctx* c, int nxp, const lynx_ctx::NLMap** out) {
+    auto it = c->nl_maps.find(nxp);
+    if (it != c->nl_maps.end()) {
+        *out = &it->second;
+        return LYNX_OK;
+    }
+    lynx_ctx::NLMap& m = c->nl_maps[nxp];
+    m.mp = (nxp + 3) & ~3;
+    const long long rows = (long long)c->ny * c->nz;
+    std::vector<int> pm((size_t)rows * m.mp, -1);
+    m.rowstart_h.assign(rows + 1, 0);
+    const std::vector<int>& pg = c->h_pt_grid;  // grid order, rows of nx
+    for (size_t p = 0; p < pg.size(); ++p) {
+        const int x = pg[p] % c->nx;
+        const long long row = pg[p] / c->nx;
+        pm[(size_t)row * m.mp + x] = (int)p;
+        m.rowstart_h[row + 1]++;
+    }
+    for (long long r = 0; r < rows; ++r) m.rowstart_h[r + 1] += m.rowstart_h[r];
+    LYNX_TRY(m.ptmap.ensure(pm.size() * sizeof(int)));
+    LYNX_CUDA_TRY(cudaMemcpy(m.ptmap.p, pm.data(), pm.size() * sizeof(int), cudaMemcpyHostToDevice));
+    LYNX_TRY(m.rowstart.ensure(m.rowstart_h.size() * sizeof(int)));
+    LYNX_CUDA_TRY(cudaMemcpy(m.rowstart.p, m.rowstart_h.data(), m.rowstart_h.size() * sizeof(int),
+                             cudaMemcpyHostToDevice));
+    *out = &m;
+    return LYNX_OK;
+}
+
 // Veff (FP64, Nd, device) in scalar type S with rows of length nxp.
 template <typename S>
 int veff_layout(lynx_ctx* c, const double* v, int nxp, const S** out) {
@@ -500,16 +540,16 @@ int check_errflag(lynx_ctx* c) {
 template <typename T, typename S>
 int pipe_launch_tuned(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out,
                       long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl,
-                      const T* phr) {
+                      const T* phr, const PipeNLHost* nlh) {
     const StencilGeom g = geom(c);
     const int nsh = pipe_shape_count<T>(g.R);
-    const std::array<long long, 6> key = {(long long)sizeof(T), (long long)ScalarOf<T>::cplx, nxp, c->ny, c->nz,
-                                          ncol};
+    const std::array<long long, 7> key = {(long long)sizeof(T), (long long)ScalarOf<T>::cplx, nxp, c->ny, c->nz,
+                                          ncol, nlh != nullptr};
     auto it = c->pipe_shape.find(key);
     if (it != c->pipe_shape.end() || nsh <= 1 || !c->autotune) {
         const int si = (it != c->pipe_shape.end()) ? it->second : 0;
         return launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
-                                      c->errflag.as<int>(), c->stream, si);
+                                      c->errflag.as<int>(), c->stream, si, nlh);
     }
     cudaEvent_t e0, e1;
     LYNX_CUDA_TRY(cudaEventCreate(&e0));
@@ -519,11 +559,11 @@ int pipe_launch_tuned(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* 
     int rc = LYNX_OK;
     for (int si = 0; si < nsh && rc == LYNX_OK; ++si) {
         rc = launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
-                                    c->errflag.as<int>(), c->stream, si);
+                                    c->errflag.as<int>(), c->stream, si, nlh);
         if (rc != LYNX_OK) break;
         cudaEventRecord(e0, c->stream);
         rc = launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
-                                    c->errflag.as<int>(), c->stream, si);
+                                    c->errflag.as<int>(), c->stream, si, nlh);
         cudaEventRecord(e1, c->stream);
         if (rc != LYNX_OK) break;
         if (cudaEventSynchronize(e1) != cudaSuccess) {
@@ -544,13 +584,19 @@ int pipe_launch_tuned(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* 
     c->pipe_shape[key] = best;
     if (best != nsh - 1)  // leave the chosen shape's (identical) output as the result of record
         return launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
-                                      c->errflag.as<int>(), c->stream, best);
+                                      c->errflag.as<int>(), c->stream, best, nlh);
     return LYNX_OK;
 }
 
+// One Chebyshev step out = a H x + b x + d xold (H with the nonlocal term when tables are set).
+// With the fused nonlocal path, xs_in (optional) is the compact sphere-point copy of x written
+// by the previous step, and xs_out (optional) receives the compact copy of out; *xs_written
+// tells the caller whether it was written (the fused path was taken).
 template <typename T>
 int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out, long long ldout,
-              const typename Real<T>::type* V, int ncol, double a, double b, double d, bool use_k) {
+              const typename Real<T>::type* V, int ncol, double a, double b, double d, bool use_k,
+              const T* xs_in = nullptr, T* xs_out = nullptr, bool* xs_written = nullptr) {
+    if (xs_written) *xs_written = false;
     using S = typename Real<T>::type;
     T phl[3], phr[3];
     ghost_phases<T>(c, use_k, phl, phr);
@@ -562,15 +608,43 @@ int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, lo
         return LYNX_ERR_BAD_ARG;
     }
     const int ncolp = ((ncol + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
+    // Fused nonlocal term: real data, periodic cell, pipelined kernel, disjoint spheres.  The
+    // values (chi alpha) are expanded to the compact point numbering and added by the stencil
+    // kernel itself (out += a * W), in the order the separate scatter would add them.
+    const bool fuse = c->has_nl && c->fuse_nl && pipe_ok && !ScalarOf<T>::cplx && !use_k && c->nl.compact &&
+                      c->nl.n_colors == 1 && geom(c).R == 6 && c->bc[0] == LYNX_BC_PERIODIC &&
+                      c->bc[1] == LYNX_BC_PERIODIC && c->bc[2] == LYNX_BC_PERIODIC;
+    const long long ldw = ((long long)c->nl.n_pts + 3) & ~3LL;  // compact column stride
     const NLDev* nl = nullptr;
     if (c->has_nl) {
         LYNX_TRY(nl_for(c, nxp, &nl));
         LYNX_TRY(c->alpha.ensure(sizeof(T) * (size_t)c->nl.total_proj * ncolp));
-        LYNX_TRY(launch_nl_gather<T>(*nl, x, ldx, ncol, c->alpha.as<T>(), ncolp, c->dV, c->stream));
+        if (fuse && xs_in) {
+            // gather from the dense compact copy: entries index it through ent_pt
+            NLDev cv = *nl;
+            cv.gpos = c->nl.ent_pt;
+            LYNX_TRY(launch_nl_gather<T>(cv, xs_in, ldw, ncol, c->alpha.as<T>(), ncolp, c->dV, c->stream));
+        } else {
+            LYNX_TRY(launch_nl_gather<T>(*nl, x, ldx, ncol, c->alpha.as<T>(), ncolp, c->dV, c->stream));
+        }
     }
     if (pipe_ok) {
         if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
-        LYNX_TRY(pipe_launch_tuned<T, S>(c, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr));
+        if constexpr (!ScalarOf<T>::cplx) {
+            if (fuse) {
+                const lynx_ctx::NLMap* nm = nullptr;
+                LYNX_TRY(nl_map_for(c, nxp, &nm));
+                LYNX_TRY(c->nlW.ensure(sizeof(T) * (size_t)ldw * ncol));
+                LYNX_TRY(launch_nl_expand<T>(*nl, c->nlW.as<T>(), ldw, ncol, c->alpha.as<T>(), ncolp, c->stream));
+                PipeNLHost nh{c->nlW.p, ldw, nm->ptmap.as<int>(), nm->mp, nm->rowstart.as<int>(), &nm->rowstart_h,
+                              xs_out};
+                LYNX_TRY(pipe_launch_tuned<T, S>(c, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
+                                                 &nh));
+                if (xs_written) *xs_written = (xs_out != nullptr);
+                return LYNX_OK;
+            }
+        }
+        LYNX_TRY(pipe_launch_tuned<T, S>(c, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, nullptr));
     } else {
         LYNX_TRY(launch_cheb_step<T, S>(geom(c), x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, c->stream));
     }
@@ -582,17 +656,37 @@ int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, lo
 // Chebyshev filter (src/solvers/EigenSolver.cpp:559-619) on blocks of type T with rows of
 // length nxp.  X (column stride ldX) is read at the first two steps only; bufs[0..2]
 // (column stride ldb) rotate.  Returns the block holding the filtered Y in *yout.
+// Compact sphere-point buffers (two, used alternately) for the fused nonlocal path; null when
+// the path does not apply.
+template <typename T>
+int compact_bufs(lynx_ctx* c, int ncol, T* xs[2]) {
+    xs[0] = xs[1] = nullptr;
+    if (ScalarOf<T>::cplx || !c->has_nl || !c->fuse_nl || !c->nl.compact || c->nl.n_colors != 1) return LYNX_OK;
+    const long long ldw = ((long long)c->nl.n_pts + 3) & ~3LL;
+    for (int i = 0; i < 2; ++i) {
+        LYNX_TRY(c->xsbuf[i].ensure(sizeof(T) * (size_t)ldw * ncol));
+        xs[i] = c->xsbuf[i].as<T>();
+    }
+    return LYNX_OK;
+}
+
 template <typename T>
 int filter_blocks(lynx_ctx* c, int nxp, const T* X, long long ldX, T* bufs[3], long long ldb,
                   const typename Real<T>::type* V, int ncol, double lc, double emin, double emax, int degree,
-                  bool use_k, T** yout) {
+                  bool use_k, T** yout, const T** ys_out = nullptr) {
     const double e = (emax - lc) / 2.0;
     const double cc = (emax + lc) / 2.0;
     const double sigma1 = e / (emin - cc);
     double sigma = sigma1;
+    T* xs[2];
+    LYNX_TRY(compact_bufs<T>(c, ncol, xs));
+    const T* xin = nullptr;  // compact copy of the current x, when the previous step wrote one
+    bool wr = false;
     // Y = (sigma1/e) (H X - c X)
     const double s0 = sigma1 / e;
-    LYNX_TRY(cheb_step<T>(c, nxp, X, ldX, nullptr, 0, bufs[0], ldb, V, ncol, s0, -cc * s0, 0.0, use_k));
+    LYNX_TRY(cheb_step<T>(c, nxp, X, ldX, nullptr, 0, bufs[0], ldb, V, ncol, s0, -cc * s0, 0.0, use_k, nullptr, xs[0],
+                          &wr));
+    xin = wr ? xs[0] : nullptr;
     const T* xold = X;
     long long ldold = ldX;
     int iy = 0;
@@ -600,14 +694,17 @@ int filter_blocks(lynx_ctx* c, int nxp, const T* X, long long ldX, T* bufs[3], l
         const double sigma_new = 1.0 / (2.0 / sigma1 - sigma);
         const double gamma = 2.0 * sigma_new / e;
         const int inew = (iy + 1) % 3;
+        T* xo = xs[(k - 1) & 1];
         LYNX_TRY(cheb_step<T>(c, nxp, bufs[iy], ldb, xold, ldold, bufs[inew], ldb, V, ncol, gamma, -gamma * cc,
-                              -sigma * sigma_new, use_k));
+                              -sigma * sigma_new, use_k, xin, xo, &wr));
+        xin = wr ? xo : nullptr;
         xold = bufs[iy];
         ldold = ldb;
         iy = inew;
         sigma = sigma_new;
     }
     *yout = bufs[iy];
+    if (ys_out) *ys_out = xin;
     return LYNX_OK;
 }
 
@@ -635,10 +732,11 @@ int run_filter64(lynx_ctx* c, const T64* X, long long ldX, const double* veff, i
         ldin = *ldb;
     }
     T64* bufs[3] = {c->wbuf[0].as<T64>(), c->wbuf[1].as<T64>(), c->wbuf[2].as<T64>()};
-    LYNX_TRY(filter_blocks<T64>(c, *nxp, Xin, ldin, bufs, *ldb, Vp, N, lc, emin, emax, degree, use_k, Y));
+    const T64* ys = nullptr;
+    LYNX_TRY(filter_blocks<T64>(c, *nxp, Xin, ldin, bufs, *ldb, Vp, N, lc, emin, emax, degree, use_k, Y, &ys));
     if (want_hy) {
         *HY = (*Y == bufs[0]) ? bufs[1] : bufs[0];
-        LYNX_TRY(cheb_step<T64>(c, *nxp, *Y, *ldb, nullptr, 0, *HY, *ldb, Vp, N, 1.0, 0.0, 0.0, use_k));
+        LYNX_TRY(cheb_step<T64>(c, *nxp, *Y, *ldb, nullptr, 0, *HY, *ldb, Vp, N, 1.0, 0.0, 0.0, use_k, ys));
     }
     return LYNX_OK;
 }
@@ -658,10 +756,11 @@ int run_filter32(lynx_ctx* c, const T64* X, long long ldX, const double* veff, i
     T32* X32 = c->wbuf[3].as<T32>();
     LYNX_TRY(repack<T32, T64>(c, X32, *nxp, *ldb, X, c->nx, ldX, N));
     T32* bufs[3] = {c->wbuf[0].as<T32>(), c->wbuf[1].as<T32>(), c->wbuf[2].as<T32>()};
-    LYNX_TRY(filter_blocks<T32>(c, *nxp, X32, *ldb, bufs, *ldb, Vp, N, lc, emin, emax, degree, use_k, Y));
+    const T32* ys = nullptr;
+    LYNX_TRY(filter_blocks<T32>(c, *nxp, X32, *ldb, bufs, *ldb, Vp, N, lc, emin, emax, degree, use_k, Y, &ys));
     if (want_hy) {
         *HY = (*Y == bufs[0]) ? bufs[1] : bufs[0];
-        LYNX_TRY(cheb_step<T32>(c, *nxp, *Y, *ldb, nullptr, 0, *HY, *ldb, Vp, N, 1.0, 0.0, 0.0, use_k));
+        LYNX_TRY(cheb_step<T32>(c, *nxp, *Y, *ldb, nullptr, 0, *HY, *ldb, Vp, N, 1.0, 0.0, 0.0, use_k, ys));
     }
     return LYNX_OK;
 }
@@ -1211,7 +1310,14 @@ int lynx_destroy(lynx_ctx* c) {
     c->errflag.release();
     c->gwork.release();
     c->rwork.release();
+    c->nlW.release();
+    c->xsbuf[0].release();
+    c->xsbuf[1].release();
     for (auto& b : c->nl_layout_bufs) b.release();
+    for (auto& kv : c->nl_maps) {
+        kv.second.ptmap.release();
+        kv.second.rowstart.release();
+    }
     if (c->cublas) cublasDestroy(c->cublas);
     if (c->cusolver) cusolverDnDestroy(c->cusolver);
     delete c;
@@ -1259,6 +1365,11 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
     for (auto& b : c->nl_layout_bufs) b.release();
     c->nl_layout_bufs.clear();
     c->nl_layouts.clear();
+    for (auto& kv : c->nl_maps) {
+        kv.second.ptmap.release();
+        kv.second.rowstart.release();
+    }
+    c->nl_maps.clear();
     c->h_gpos.clear();
     c->h_pt_grid.clear();
     c->nl = NLDev();
@@ -1364,7 +1475,7 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
         *dst = b.p;
         return LYNX_OK;
     };
-    c->nl_bufs.reserve(24);
+    c->nl_bufs.reserve(32);
     NLDev& d = c->nl;
     d.n_atom = n_atom;
     d.n_img = n_img;
@@ -1391,6 +1502,31 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
     LYNX_TRY(up(ent_img.data(), ent_img.size() * 4, (void**)&d.ent_img));
     LYNX_TRY(up(ent_loc.data(), ent_loc.size() * 4, (void**)&d.ent_loc));
     d.n_colors = n_colors;
+    {
+        // compact numbering: distinct points in grid order; every entry its own point
+        d.compact = ((long long)pt_grid.size() == tot);
+        if (d.compact) {
+            std::vector<int> ent_pt(tot), pt_meta(2 * tot);
+            std::vector<double> cp64((size_t)max_np * tot, 0.0);
+            std::vector<float> cp32((size_t)max_np * tot, 0.0f);
+            for (long long s2 = 0; s2 < tot; ++s2) {
+                const long long k = keys[s2] & 0xFFFFFFFFLL;  // entry (image-major) of point s2
+                ent_pt[k] = (int)s2;
+                const int im = owner_img[k], l = owner_loc[k], a = img_atom[im];
+                pt_meta[2 * s2] = poff[a];
+                pt_meta[2 * s2 + 1] = nproj[a];
+                for (int j = 0; j < nproj[a]; ++j) {
+                    const double v = chi[choff[im] + (long long)j * img_ndc[im] + l];
+                    cp64[(size_t)j * tot + s2] = v;
+                    cp32[(size_t)j * tot + s2] = (float)v;
+                }
+            }
+            LYNX_TRY(up(ent_pt.data(), ent_pt.size() * 4, (void**)&d.ent_pt));
+            LYNX_TRY(up(pt_meta.data(), pt_meta.size() * 4, (void**)&d.pt_meta));
+            LYNX_TRY(up(cp64.data(), cp64.size() * 8, (void**)&d.chi_pt64));
+            LYNX_TRY(up(cp32.data(), cp32.size() * 4, (void**)&d.chi_pt32));
+        }
+    }
     if (n_colors > 0) {
         for (int k = 0, o = 0; k < n_colors; ++k) {
             d.color_off[k] = o;
@@ -1698,6 +1834,15 @@ int noalloc_scratch(int device, void** out) {
     return LYNX_OK;
 }
 }  // namespace
+
+extern "C" int lynx_set_option(lynx_ctx* c, int option, int value) {
+    LYNX_CHECK_ARG(c != nullptr, "null context");
+    switch (option) {
+        case LYNX_OPT_AUTOTUNE: c->autotune = value != 0; return LYNX_OK;
+        case LYNX_OPT_FUSE_NONLOCAL: c->fuse_nl = value != 0; return LYNX_OK;
+        default: set_error("unknown option %d", option); return LYNX_ERR_BAD_ARG;
+    }
+}
 
 extern "C" int lynx_nonlocal_apply_noalloc(lynx_ctx* c, const double* psi, double* hpsi, int ncol, int ld) {
     LYNX_CHECK_ARG(c && psi && hpsi, "null pointer");

@@ -237,11 +237,34 @@ struct Gather2Geom {
     static constexpr int CSP = 2 * NPGP;                   // chi row stride
     static constexpr size_t xs_elems = (size_t)kNL2Pts * kNL2Cols;
     static constexpr size_t cs_elems = (size_t)kNL2Pts * CSP;
+    static constexpr size_t buf_elems = xs_elems + cs_elems;        // one tile buffer
     static constexpr size_t red_elems = (size_t)4 * 32 * 4 * NPG;  // 4 warps x 32 lanes x accumulators
     static constexpr size_t smem_bytes =
-        sizeof(T) * ((xs_elems + cs_elems) > red_elems ? (xs_elems + cs_elems) : red_elems);
+        sizeof(T) * ((2 * buf_elems) > red_elems ? (2 * buf_elems) : red_elems);
 };
 
+// Asynchronous 4- or 8-byte global -> shared copy; src_bytes = 0 fills the destination with
+// zeros without reading the source.
+template <int BYTES>
+__device__ __forceinline__ void cp_async_small(void* dst, const void* src, int src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(
+                     static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src), "n"(BYTES), "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Position in an atom's tile sequence: image ii of the atom, first point g0 of the tile.
+struct TileIt {
+    int ii, g0;
+};
+
+// Tiles are double-buffered: the asynchronous copies of tile t+1 are issued before the FMAs of
+// tile t, so the gathered loads of one tile overlap the arithmetic of the previous one.
 template <typename T, int NPG>
 __global__ void __launch_bounds__(256)
     nl_gather2_kernel(const T* __restrict__ x, long long ld, int ncol, int ncolp, NLView tab, T* __restrict__ alpha,
@@ -249,13 +272,14 @@ __global__ void __launch_bounds__(256)
     using Geo = Gather2Geom<T, NPG>;
     constexpr int NB = kNL2Cols, G = kNL2Pts, NPGP = Geo::NPGP, CSP = Geo::CSP;
     extern __shared__ __align__(16) unsigned char smraw[];
-    T* xs = reinterpret_cast<T*>(smraw);  // [G][NB], 4-column groups swizzled by (g & 7)
-    T* cs = xs + Geo::xs_elems;           // [G][CSP]
+    // two tile buffers, each [G][NB] x (4-column groups swizzled by g & 7) then [G][CSP] chi
+    T* const buf0 = reinterpret_cast<T*>(smraw);
     const T* chi = reinterpret_cast<const T*>(tab.chi);
     const int a = blockIdx.x;
     const int n0 = blockIdx.y * NB;
     const int np = tab.atom_nproj[a];
     const int poff = tab.atom_poff[a];
+    const int ii_end = tab.atom_img_ptr[a + 1];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int cg = lane & 15, pg = lane >> 4;
     T acc[4][NPG];
@@ -263,66 +287,96 @@ __global__ void __launch_bounds__(256)
     for (int k = 0; k < 4; ++k)
 #pragma unroll
         for (int m = 0; m < NPG; ++m) acc[k][m] = T(0);
-    for (int ii = tab.atom_img_ptr[a]; ii < tab.atom_img_ptr[a + 1]; ++ii) {
-        const int im = tab.atom_img_list[ii];
+
+    auto normalize = [&](TileIt t) {  // first non-empty tile at or after (ii, g0)
+        while (t.ii < ii_end && t.g0 >= tab.img_ndc[tab.atom_img_list[t.ii]]) {
+            ++t.ii;
+            t.g0 = 0;
+        }
+        return t;
+    };
+    auto issue = [&](TileIt t, int bi) {  // asynchronous copies of tile t into buffer bi
+        T* xs = buf0 + (size_t)bi * Geo::buf_elems;
+        T* cs = xs + Geo::xs_elems;
+        const int im = tab.atom_img_list[t.ii];
         const int ndc = tab.img_ndc[im];
-        const int* gp = tab.gpos + tab.img_goff[im];
-        const T* ch = chi + tab.img_chi_off[im];
-        for (int g0 = 0; g0 < ndc; g0 += G) {
-            const int gl = min(G, ndc - g0);
-            __syncthreads();
+        const int gl = min(G, ndc - t.g0);
+        const int* gp = tab.gpos + tab.img_goff[im] + t.g0;
+        const T* ch = chi + tab.img_chi_off[im] + t.g0;
 #pragma unroll
-            for (int pp = 0; pp < 2; ++pp) {
-                const int g = lane + 32 * pp;
-                const bool okg = g < gl;
-                const long long base = okg ? (long long)gp[g0 + g] : 0;
+        for (int pp = 0; pp < 2; ++pp) {
+            const int g = lane + 32 * pp;
+            const bool okg = g < gl;
+            const long long base = okg ? (long long)gp[g] : 0;
 #pragma unroll
-                for (int qq = 0; qq < 2; ++qq) {
-                    const int q = w + 8 * qq;
-                    T v[4];
+            for (int qq = 0; qq < 2; ++qq) {
+                const int q = w + 8 * qq;
+                T* dst = xs + g * NB + 4 * (q ^ (g & 7));
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        const int col = n0 + 4 * q + k;
-                        v[k] = (okg && col < ncol) ? x[base + (long long)col * ld] : T(0);
-                    }
-                    store_vec4(xs + g * NB + 4 * (q ^ (g & 7)), v);
+                for (int k = 0; k < 4; ++k) {
+                    const int col = n0 + 4 * q + k;
+                    const bool ok = okg && col < ncol;
+                    cp_async_small<sizeof(T)>(dst + k, x + (ok ? base + (long long)col * ld : 0),
+                                              ok ? (int)sizeof(T) : 0);
                 }
-            }
-            for (int e = tid; e < G * CSP; e += 256) {
-                const int g = e % G, sl = e / G;
-                const int gq = sl / NPGP, m = sl % NPGP;
-                const int j = gq * NPG + m;
-                cs[g * CSP + sl] = (g < gl && m < NPG && j < np) ? ch[(long long)j * ndc + g0 + g] : T(0);
-            }
-            __syncthreads();
-            for (int g = w; g < gl; g += 8) {
-                T xv[4];
-                load_vec4(xs + g * NB + 4 * (cg ^ (g & 7)), xv);
-                const T* cp = cs + g * CSP + pg * NPGP;
-                T cv[NPGP];
-                if constexpr (sizeof(T) == 4) {
-#pragma unroll
-                    for (int m = 0; m < NPGP; m += 4) {
-                        const float4 q = *reinterpret_cast<const float4*>(cp + m);
-                        cv[m] = q.x;
-                        cv[m + 1] = q.y;
-                        cv[m + 2] = q.z;
-                        cv[m + 3] = q.w;
-                    }
-                } else {
-#pragma unroll
-                    for (int m = 0; m < NPGP; m += 2) {
-                        const double2 q = *reinterpret_cast<const double2*>(cp + m);
-                        cv[m] = q.x;
-                        cv[m + 1] = q.y;
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-#pragma unroll
-                    for (int m = 0; m < NPG; ++m) acc[k][m] = fma(cv[m], xv[k], acc[k][m]);
             }
         }
+        for (int e = tid; e < G * CSP; e += 256) {
+            const int g = e % G, sl = e / G;
+            const int gq = sl / NPGP, m = sl % NPGP;
+            const int j = gq * NPG + m;
+            const bool ok = g < gl && m < NPG && j < np;
+            cp_async_small<sizeof(T)>(cs + g * CSP + sl, ch + (ok ? (long long)j * ndc + g : 0),
+                                      ok ? (int)sizeof(T) : 0);
+        }
+        cp_async_commit();
+    };
+
+    TileIt cur = normalize(TileIt{tab.atom_img_ptr[a], 0});
+    int bi = 0;
+    if (cur.ii < ii_end) issue(cur, 0);
+    while (cur.ii < ii_end) {
+        const int gl = min(G, tab.img_ndc[tab.atom_img_list[cur.ii]] - cur.g0);
+        const TileIt nxt = normalize(TileIt{cur.ii, cur.g0 + G});
+        if (nxt.ii < ii_end) {
+            issue(nxt, bi ^ 1);  // that buffer was released by the barrier that ended the last tile
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const T* xs = buf0 + (size_t)bi * Geo::buf_elems;
+        const T* cs = xs + Geo::xs_elems;
+        for (int g = w; g < gl; g += 8) {
+            T xv[4];
+            load_vec4(xs + g * NB + 4 * (cg ^ (g & 7)), xv);
+            const T* cp = cs + g * CSP + pg * NPGP;
+            T cv[NPGP];
+            if constexpr (sizeof(T) == 4) {
+#pragma unroll
+                for (int m = 0; m < NPGP; m += 4) {
+                    const float4 q = *reinterpret_cast<const float4*>(cp + m);
+                    cv[m] = q.x;
+                    cv[m + 1] = q.y;
+                    cv[m + 2] = q.z;
+                    cv[m + 3] = q.w;
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < NPGP; m += 2) {
+                    const double2 q = *reinterpret_cast<const double2*>(cp + m);
+                    cv[m] = q.x;
+                    cv[m + 1] = q.y;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int m = 0; m < NPG; ++m) acc[k][m] = fma(cv[m], xv[k], acc[k][m]);
+        }
+        __syncthreads();  // every warp is done with buffer bi before it is refilled
+        cur = nxt;
+        bi ^= 1;
     }
     // fixed-order tree over the 8 warps: 4+4, 2+2, 1+1
     T* red = reinterpret_cast<T*>(smraw);
@@ -361,10 +415,13 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-template <typename T>
+// COMPACT: instead of out[gpos] += scale * (chi alpha), store chi alpha into the compact
+// per-point array out[col * ld + ent_pt[entry]] (every grid point has exactly one entry).
+template <typename T, bool COMPACT = false>
 __global__ void __launch_bounds__(256)
     nl_scatter2_kernel(T* __restrict__ out, long long ld, int ncol, int ncolp, NLView tab,
-                       const int* __restrict__ imgs, const T* __restrict__ alpha, T scale) {
+                       const int* __restrict__ imgs, const T* __restrict__ alpha, T scale,
+                       const int* __restrict__ ent_pt = nullptr) {
     constexpr int NB = kNL2Cols, G = kNL2Pts;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int im = imgs[blockIdx.x];
@@ -415,16 +472,88 @@ __global__ void __launch_bounds__(256)
         for (int p = 0; p < 2; ++p) {
             const int g = g0 + lane + 32 * p;
             if (g < ndc) {
-                T* o = out + gp[g];
+                if constexpr (COMPACT) {
+                    T* o = out + ent_pt[tab.img_goff[im] + g];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int col = n0 + 8 * w + k;
-                    if (col < ncol) {
-                        T* q = o + (long long)col * ld;
-                        *q = fma(scale, acc[p][k], *q);
+                    for (int k = 0; k < 8; ++k) {
+                        const int col = n0 + 8 * w + k;
+                        if (col < ncol) o[(long long)col * ld] = acc[p][k];
+                    }
+                } else {
+                    T* o = out + gp[g];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const int col = n0 + 8 * w + k;
+                        if (col < ncol) {
+                            T* q = o + (long long)col * ld;
+                            *q = fma(scale, acc[p][k], *q);
+                        }
                     }
                 }
             }
+        }
+    }
+}
+
+// expand on the compact numbering, point-major: W[col * ldw + pt] = sum_j chi_pt[j][pt] *
+// alpha[(poff(atom(pt)) + j) * ncolp + col], summed over j in increasing order (the order the
+// scatter kernels use).  CTA = 64 consecutive points x 64 columns, 256 threads: warp w owns
+// columns 8w..8w+7, lane owns points lane and lane + 32, so every store instruction writes a
+// contiguous run of W.
+template <typename T>
+__global__ void __launch_bounds__(256)
+    nl_expand_pt_kernel(T* __restrict__ W, long long ldw, int ncol, int ncolp, int n_pts,
+                        const T* __restrict__ chi_pt, const int2* __restrict__ pt_meta, const T* __restrict__ alpha) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int n0 = blockIdx.y * kNL2Cols + 8 * w;
+    const int ptA = blockIdx.x * kNL2Pts + lane, ptB = ptA + 32;
+    // pt_meta[pt] = (first projector row of the point's atom, projector count)
+    const int2 mA = (ptA < n_pts) ? pt_meta[ptA] : make_int2(0, 0);
+    const int2 mB = (ptB < n_pts) ? pt_meta[ptB] : make_int2(0, 0);
+    const T* alA = alpha + (long long)mA.x * ncolp + n0;
+    const T* alB = alpha + (long long)mB.x * ncolp + n0;
+    const bool full = n0 + 8 <= ncolp;
+    T accA[8], accB[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) accA[k] = accB[k] = T(0);
+    auto row8 = [&](const T* al, int j, T (&v)[8]) {
+        if (full) {
+            T t0[4], t1[4];
+            load_vec4(al + (long long)j * ncolp, t0);
+            load_vec4(al + (long long)j * ncolp + 4, t1);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                v[k] = t0[k];
+                v[k + 4] = t1[k];
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = (n0 + k < ncolp) ? al[(long long)j * ncolp + k] : T(0);
+        }
+    };
+    const int npm = max(mA.y, mB.y);
+#pragma unroll 2
+    for (int j = 0; j < npm; ++j) {
+        if (j < mA.y) {
+            const T c = chi_pt[(long long)j * n_pts + ptA];
+            T v[8];
+            row8(alA, j, v);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) accA[k] = fma(c, v[k], accA[k]);
+        }
+        if (j < mB.y) {
+            const T c = chi_pt[(long long)j * n_pts + ptB];
+            T v[8];
+            row8(alB, j, v);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) accB[k] = fma(c, v[k], accB[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (n0 + k < ncol) {
+            if (ptA < n_pts) W[(long long)(n0 + k) * ldw + ptA] = accA[k];
+            if (ptB < n_pts) W[(long long)(n0 + k) * ldw + ptB] = accB[k];
         }
     }
 }

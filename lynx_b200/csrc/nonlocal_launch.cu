@@ -135,6 +135,29 @@ int launch_nl_scatter(const NLDev& nl, T* out, long long ld, int ncol, const T* 
     return LYNX_OK;
 }
 
+template <typename T>
+int launch_nl_expand(const NLDev& nl, T* W, long long ldw, int ncol, const T* alpha, int ncolp, cudaStream_t st) {
+    if constexpr (kReal<T>) {
+        if (!nl.compact || nl.n_colors != 1 || nl.max_np > 32) {
+            set_error("compact nonlocal expansion needs disjoint projector spheres");
+            return LYNX_ERR_UNSUPPORTED;
+        }
+        if (nl.n_pts == 0 || ncol <= 0) return LYNX_OK;
+        const T* chi_pt;
+        if constexpr (std::is_same<T, float>::value) chi_pt = nl.chi_pt32;
+        else chi_pt = nl.chi_pt64;
+        dim3 grid((nl.n_pts + kNL2Pts - 1) / kNL2Pts, (ncol + kNL2Cols - 1) / kNL2Cols);
+        nl_expand_pt_kernel<T><<<grid, 256, 0, st>>>(W, ldw, ncol, ncolp, nl.n_pts, chi_pt, nl.pt_meta, alpha);
+        count_launch();
+        return launch_status("nonlocal expansion");
+    } else {
+        set_error("compact nonlocal expansion is for real data");
+        return LYNX_ERR_UNSUPPORTED;
+    }
+}
+
+template int launch_nl_expand<double>(const NLDev&, double*, long long, int, const double*, int, cudaStream_t);
+template int launch_nl_expand<float>(const NLDev&, float*, long long, int, const float*, int, cudaStream_t);
 template int launch_nl_gather<double>(const NLDev&, const double*, long long, int, double*, int, double, cudaStream_t);
 template int launch_nl_gather<float>(const NLDev&, const float*, long long, int, float*, int, double, cudaStream_t);
 template int launch_nl_gather<double2>(const NLDev&, const double2*, long long, int, double2*, int, double, cudaStream_t);

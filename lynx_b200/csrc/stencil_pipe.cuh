@@ -58,6 +58,38 @@ struct PipeCoef {
     T phl[3], phr[3];
 };
 
+// Fused nonlocal term (real data, disjoint projector spheres): W holds (chi alpha) per sphere
+// point in grid order (column stride ldw); ptmap (row pitch mp, same rows as the grid) gives
+// each grid point's number in that order, or -1; rowstart[z * ny + y] is the number of the
+// first sphere point at or after row (z, y).  wcap: the largest W range of one band-plane,
+// rounded out to 16-byte boundaries.
+template <typename T>
+struct PipeNL {
+    const T* W;
+    long long ldw;
+    const int* ptmap;
+    int mp;
+    const int* rowstart;
+    int wcap;
+    T* xs_out;  // optional: compact copy of out at the sphere points (column stride ldw)
+};
+
+// Byte layout of one tile stage: [tile rows][xold rows][Veff rows][ptmap rows][W range],
+// every part 16-byte aligned; returns the 128-byte rounded stage size.
+struct StageLayout {
+    int v_off, pm_off, w_off, bytes;
+};
+__host__ __device__ inline StageLayout pipe_stage_layout(int TY, int R, int nxp, int szT, int szS, bool xold, bool nlf,
+                                                        int mp, int wcap) {
+    StageLayout L;
+    const int tb = ((TY + 2 * R) * nxp + (xold ? TY * nxp : 0)) * szT;
+    L.v_off = (tb + 15) & ~15;
+    L.pm_off = (L.v_off + TY * nxp * szS + 15) & ~15;
+    L.w_off = (L.pm_off + (nlf ? TY * mp * 4 : 0) + 15) & ~15;
+    L.bytes = ((L.w_off + (nlf ? wcap * szT : 0) + 127) / 128) * 128;
+    return L;
+}
+
 template <typename T, int RX> struct VecOf { using type = T; };
 template <> struct VecOf<float, 2> { using type = float2; };
 template <> struct VecOf<double, 2> { using type = double2; };
@@ -121,16 +153,16 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 // through column offsets wrapped once at start-up, and PHASED instantiations (Bloch phases,
 // Dirichlet zeros) multiply wrapped neighbours in registers.  Per stage two mbarriers:
 // full (copies landed, tx-counted) and empty (every consumer warp done reading).
-template <typename T, int R, int RX, int RY, bool XOLD, int NS, bool PHASED, int MAXT>
+template <typename T, int R, int RX, int RY, bool XOLD, int NS, bool PHASED, int MAXT, bool NLF>
 __global__ void __launch_bounds__(MAXT, 1)
     cheb_pipe_kernel(const T* __restrict__ x, const T* __restrict__ xold, T* __restrict__ out,
                      const typename ScalarOf<T>::type* __restrict__ V, const PipeGeom G, const PipeCoef<T> C,
-                     int* __restrict__ err) {
+                     const PipeNL<T> NL, int* __restrict__ err) {
     using S = typename ScalarOf<T>::type;
     using VT = typename VecOf<T, RX>::type;
     constexpr int W = 2 * R + 1;
     constexpr int DW = 4;  // window ring depth
-    static_assert((2 * NS + 2 * DW) * 8 <= 256, "ring size out of range");
+    static_assert((2 * NS + 2 * DW) * 8 <= 192 && NS <= 16, "ring size out of range");  // 192..255: W offsets
     // x-neighbour vector loads: first element index rounded down to a multiple of RX
     constexpr int XOFF = (R % RX == 0) ? R : (R + RX - (R % RX));  // XOFF >= R, XOFF % RX == 0
     constexpr int NXV = (XOFF + R + RX + RX - 1) / RX;            // vectors covering x-XOFF .. x+RX-1+R
@@ -160,15 +192,22 @@ __global__ void __launch_bounds__(MAXT, 1)
     uint64_t* wfull = empty + NS;
     uint64_t* wempty = wfull + DW;
     T* stage0 = reinterpret_cast<T*>(smpipe + 256);
-    const int stage_bytes_T = (tile_elems + (XOLD ? own_elems : 0)) * (int)sizeof(T);
-    const int stage_stride = ((stage_bytes_T + own_elems * (int)sizeof(S) + 127) / 128) * 128;
+    int* walign = reinterpret_cast<int*>(smpipe + 192);  // per stage: first W element staged
+    const StageLayout SL = pipe_stage_layout(G.TY, R, nxp, (int)sizeof(T), (int)sizeof(S), XOLD, NLF, NL.mp, NL.wcap);
+    const int stage_stride = SL.bytes;
     const int wstage_stride = ((own_elems * (int)sizeof(T) + 127) / 128) * 128;
     auto tile_of = [&](int st) {
         return reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(stage0) + st * stage_stride);
     };
     auto xold_of = [&](int st) { return tile_of(st) + tile_elems; };
     auto veff_of = [&](int st) {
-        return reinterpret_cast<S*>(reinterpret_cast<unsigned char*>(tile_of(st)) + stage_bytes_T);
+        return reinterpret_cast<S*>(reinterpret_cast<unsigned char*>(tile_of(st)) + SL.v_off);
+    };
+    auto pm_of = [&](int st) {
+        return reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(tile_of(st)) + SL.pm_off);
+    };
+    auto wnl_of = [&](int st) {
+        return reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(tile_of(st)) + SL.w_off);
     };
     auto wstage_of = [&](int st) {
         return reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(stage0) + NS * stage_stride + st * wstage_stride);
@@ -189,6 +228,18 @@ __global__ void __launch_bounds__(MAXT, 1)
 
     if (tid >= NC) {
         // ------------------------------ producer warp ------------------------------
+        // W ranges of this band on every plane of the chunk, read once by the whole warp
+        // (after the window ring): rsv[2i], rsv[2i+1] = first / end compact point of plane z0+i.
+        int* rsv = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(stage0) + NS * stage_stride +
+                                          DW * wstage_stride);
+        if constexpr (NLF) {
+            for (int i = tid - NC; i < nplanes; i += 32) {
+                const long long rb = (long long)(z0 + i) * ny + y0;
+                rsv[2 * i] = NL.rowstart[rb];
+                rsv[2 * i + 1] = NL.rowstart[rb + TYv];
+            }
+            __syncwarp();
+        }
         if (tid != NC) return;  // one elected thread issues every copy
         const uint32_t rowb = (uint32_t)(nxp * sizeof(T));
         const uint32_t ownb = (uint32_t)(TYv * nxp * sizeof(T));
@@ -218,7 +269,19 @@ __global__ void __launch_bounds__(MAXT, 1)
                 atomicExch(err, 1);
                 return;
             }
-            mbar_expect_tx(&full[st], total);
+            uint32_t extra = 0, pmb = 0, wnb = 0;
+            int wal = 0;
+            if constexpr (NLF) {
+                constexpr int VWn = 16 / (int)sizeof(T);
+                const int ps = rsv[2 * i], pe = rsv[2 * i + 1];
+                wal = ps & ~(VWn - 1);
+                const int wae = (pe + VWn - 1) & ~(VWn - 1);
+                walign[st] = wal;  // published to the consumers by the arrive below
+                pmb = (uint32_t)(TYv * NL.mp * 4);
+                wnb = (uint32_t)((wae - wal) * (int)sizeof(T));
+                extra = pmb + wnb;
+            }
+            mbar_expect_tx(&full[st], total + extra);
             T* tile = tile_of(st);
             const T* plane = xc + (long long)z * G.plane;
             for (int q = 0; q < nruns; ++q)
@@ -226,6 +289,10 @@ __global__ void __launch_bounds__(MAXT, 1)
             const long long own0 = (long long)z * G.plane + (long long)y0 * nxp;
             if (XOLD) bulk_g2s(xold_of(st), xoc + own0, ownb, &full[st]);
             bulk_g2s(veff_of(st), V + own0, vb, &full[st]);
+            if constexpr (NLF) {
+                bulk_g2s(pm_of(st), NL.ptmap + ((long long)z * ny + y0) * NL.mp, pmb, &full[st]);
+                if (wnb) bulk_g2s(wnl_of(st), NL.W + col * NL.ldw + wal, wnb, &full[st]);
+            }
             // rows of the plane that enters the consumers' z-window after iteration i
             if (i + 1 < nplanes) {
                 const int wst = i % DW, wk = i / DW;
@@ -365,7 +432,7 @@ __global__ void __launch_bounds__(MAXT, 1)
     // Every output element sees exactly the scalar path's operations in the same order, so the
     // results are bitwise identical; the instruction count of the z, y, V and x_old terms and of
     // the even x offsets halves.
-    auto packed_plane = [&](auto Jc, int z, const T* tile, const T* xo_s, const S* v_s) {
+    auto packed_plane = [&](auto Jc, int z, int st, const T* tile, const T* xo_s, const S* v_s) {
         if constexpr (kPacked) {
             constexpr int J = decltype(Jc)::value;
             float2 acc[RY];
@@ -434,6 +501,17 @@ __global__ void __launch_bounds__(MAXT, 1)
                 const float2 vv = *reinterpret_cast<const float2*>(v_s + so);
                 acc[r] = __ffma2_rn(__fmul2_rn(make_float2(C.a, C.a), vv), w[J + R][r], acc[r]);
                 if (XOLD) acc[r] = __ffma2_rn(make_float2(C.d, C.d), *reinterpret_cast<const float2*>(xo_s + so), acc[r]);
+                if constexpr (NLF) {
+                    const int2 m = *reinterpret_cast<const int2*>(pm_of(st) + yl[r] * NL.mp + xb);
+                    const float* wn = wnl_of(st) - walign[st];
+                    if (m.x >= 0) acc[r].x = fmaf(C.a, wn[m.x], acc[r].x);
+                    if (m.y >= 0) acc[r].y = fmaf(C.a, wn[m.y], acc[r].y);
+                    if (NL.xs_out) {
+                        float* xs = NL.xs_out + col * NL.ldw;
+                        if (m.x >= 0) xs[m.x] = acc[r].x;
+                        if (m.y >= 0) xs[m.y] = acc[r].y;
+                    }
+                }
                 float* op = oc + (long long)z * G.plane + (long long)(y0 + yl[r]) * nxp + xb;
                 *reinterpret_cast<float2*>(op) = acc[r];
             }
@@ -450,7 +528,7 @@ __global__ void __launch_bounds__(MAXT, 1)
         const T* xo_s = XOLD ? xold_of(st) : nullptr;
         const S* v_s = veff_of(st);
         if constexpr (kPacked) {
-            packed_plane(Jc, z, tile, xo_s, v_s);
+            packed_plane(Jc, z, st, tile, xo_s, v_s);
         } else {
         T acc[RY][RX];
         // centre, z neighbours
@@ -538,6 +616,18 @@ __global__ void __launch_bounds__(MAXT, 1)
                 for (int u = 0; u < RX; ++u) {
                     acc[r][u] = fmac(acc[r][u], C.a * vv[u], wc[u]);
                     if (XOLD) acc[r][u] = fmac(acc[r][u], C.d, xo_e[u]);
+                }
+            }
+            if constexpr (NLF) {
+                const int* pmr = pm_of(st) + yl[r] * NL.mp + xb;
+                const T* wn = wnl_of(st) - walign[st];
+#pragma unroll
+                for (int u = 0; u < RX; ++u) {
+                    const int m = pmr[u];
+                    if (m >= 0) {
+                        acc[r][u] = fmac(acc[r][u], C.a, wn[m]);
+                        if (NL.xs_out) NL.xs_out[col * NL.ldw + m] = acc[r][u];
+                    }
                 }
             }
             T* op = oc + (long long)z * G.plane + (long long)(y0 + yl[r]) * nxp + xb;

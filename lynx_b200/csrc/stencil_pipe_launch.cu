@@ -53,37 +53,46 @@ ShapeRT shape_rt(int si) {
     return shape_i<T, 0>();
 }
 
-template <typename T, int R, bool XOLD, bool PH, int SI>
+template <typename T, int R, bool XOLD, bool PH, int SI, bool NLF = false>
 void launch_pipe_ph(int ns, dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x, const T* xo, T* out,
-                    const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C, int* err) {
+                    const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C,
+                    const PipeNL<T>& NL, int* err) {
     using P = PipeShapeAt<T, SI>;
     constexpr int RX = P::RX, RY = P::RY, MT = P::MAXT;
-    auto kern = ns >= 5 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 5, PH, MT>
-               : (ns == 4 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 4, PH, MT>
-                          : cheb_pipe_kernel<T, R, RX, RY, XOLD, 3, PH, MT>);
+    auto kern = ns >= 5 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 5, PH, MT, NLF>
+               : (ns == 4 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 4, PH, MT, NLF>
+                          : cheb_pipe_kernel<T, R, RX, RY, XOLD, 3, PH, MT, NLF>);
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kern<<<grid, nthr, smem, st>>>(x, xo, out, V, G, C, err);
+    kern<<<grid, nthr, smem, st>>>(x, xo, out, V, G, C, NL, err);
 }
 
 // Real data with periodic boundaries needs no phase on wrapped neighbours; complex data and
 // Dirichlet boundaries use the PHASED instantiation (default shape only).
 template <typename T, int R, bool XOLD>
-void launch_pipe(int si, int ns, bool phased, dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x,
+void launch_pipe(int si, int ns, bool phased, bool nlf, dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x,
                  const T* xo, T* out, const typename ScalarOf<T>::type* V, const PipeGeom& G, const PipeCoef<T>& C,
-                 int* err) {
+                 const PipeNL<T>& NL, int* err) {
     if (ScalarOf<T>::cplx || phased) {
-        launch_pipe_ph<T, R, XOLD, true, 0>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err);
+        launch_pipe_ph<T, R, XOLD, true, 0>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, NL, err);
         return;
     }
     if constexpr (R == kTunedR && NumShapes<T>::value > 1) {
+        if (nlf) {
+            switch (si) {
+                case 1: launch_pipe_ph<T, R, XOLD, false, 1, true>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, NL, err); return;
+                case 2: launch_pipe_ph<T, R, XOLD, false, 2, true>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, NL, err); return;
+                case 3: launch_pipe_ph<T, R, XOLD, false, 3, true>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, NL, err); return;
+                default: launch_pipe_ph<T, R, XOLD, false, 0, true>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, NL, err); return;
+            }
+        }
         switch (si) {
-            case 1: launch_pipe_ph<T, R, XOLD, false, 1>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err); return;
-            case 2: launch_pipe_ph<T, R, XOLD, false, 2>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err); return;
-            case 3: launch_pipe_ph<T, R, XOLD, false, 3>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err); return;
+            case 1: launch_pipe_ph<T, R, XOLD, false, 1>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, NL, err); return;
+            case 2: launch_pipe_ph<T, R, XOLD, false, 2>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, NL, err); return;
+            case 3: launch_pipe_ph<T, R, XOLD, false, 3>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, NL, err); return;
             default: break;
         }
     }
-    launch_pipe_ph<T, R, XOLD, false, 0>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, err);
+    launch_pipe_ph<T, R, XOLD, false, 0>(ns, grid, nthr, smem, st, x, xo, out, V, G, C, NL, err);
 }
 
 template <typename T>
@@ -108,10 +117,15 @@ int pipe_shape_count(int R) {
 template <typename T, typename S>
 int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out,
                      long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl, const T* phr,
-                     int* err, cudaStream_t st, int shape) {
+                     int* err, cudaStream_t st, int shape, const PipeNLHost* nlh) {
     static_assert(std::is_same<S, typename ScalarOf<T>::type>::value, "scalar type mismatch");
     const int R = g.R;
     const bool phased = ScalarOf<T>::cplx || !phases_trivial(phl, phr);
+    const bool nlf = nlh != nullptr;
+    if (nlf && (R != kTunedR || phased || NumShapes<T>::value == 1)) {
+        set_error("fused nonlocal term needs real data, periodic cells and FD order 12");
+        return LYNX_ERR_UNSUPPORTED;
+    }
     const int si = (shape > 0 && shape < pipe_shape_count<T>(R) && !phased) ? shape : 0;
     const ShapeRT sh = shape_rt<T>(si);
     const int RX = sh.RX, RY = sh.RY, MT = sh.MAXT;
@@ -170,12 +184,31 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
     G.zchunk = (g.nz + nzch - 1) / nzch;
     nzch = (g.nz + G.zchunk - 1) / G.zchunk;
     const bool xo = (xold != nullptr) && d != 0.0;
-    const size_t tile_b = (size_t)(G.TY + 2 * R) * nxp * sizeof(T);
     const size_t own_b = (size_t)G.TY * nxp * sizeof(T);
-    const size_t v_b = (size_t)G.TY * nxp * sizeof(S);
-    const size_t stage = ((tile_b + (xo ? own_b : 0) + v_b + 127) / 128) * 128;
+    PipeNL<T> NL{};
+    if (nlf) {
+        NL.W = static_cast<const T*>(nlh->W);
+        NL.ldw = nlh->ldw;
+        NL.ptmap = nlh->ptmap;
+        NL.mp = nlh->mp;
+        NL.rowstart = nlh->rowstart;
+        NL.xs_out = static_cast<T*>(nlh->xs_out);
+        // largest 16-byte-rounded W range of one band-plane for this band height
+        const int VWn = 16 / (int)sizeof(T);
+        const std::vector<int>& rs = *nlh->rowstart_host;
+        int wcap = 0;
+        for (int z = 0; z < g.nz; ++z)
+            for (int y0 = 0; y0 < g.ny; y0 += G.TY) {
+                const int tyv = std::min(G.TY, g.ny - y0);
+                const int ps = rs[(size_t)z * g.ny + y0], pe = rs[(size_t)z * g.ny + y0 + tyv];
+                wcap = std::max(wcap, ((pe + VWn - 1) & ~(VWn - 1)) - (ps & ~(VWn - 1)));
+            }
+        NL.wcap = wcap;
+    }
+    const size_t stage = (size_t)pipe_stage_layout(G.TY, R, nxp, (int)sizeof(T), (int)sizeof(S), xo, nlf, NL.mp,
+                                                   NL.wcap).bytes;
     // window ring (4 stages of the band's own rows) + as many tile stages (3..5) as fit
-    const size_t wring = 4 * ((own_b + 127) / 128) * 128;
+    const size_t wring = 4 * ((own_b + 127) / 128) * 128 + (nlf ? (size_t)8 * G.zchunk : 0);  // + W range table
     int ns = (int)std::min<size_t>(5, (227 * 1024 - 256 - wring) / stage);
     const size_t smem = 256 + wring + (size_t)std::max(ns, 3) * stage;
     if (smem > 227 * 1024) {
@@ -203,8 +236,8 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
     dim3 grid(nbands, ncol, nzch);
 #define LYNX_PIPE_CASE(RR)                                                                       \
     case RR:                                                                                     \
-        if (xo) launch_pipe<T, RR, true>(si, ns, phased, grid, nthr, smem, st, x, xold, out, V, G, C, err);   \
-        else launch_pipe<T, RR, false>(si, ns, phased, grid, nthr, smem, st, x, xold, out, V, G, C, err);     \
+        if (xo) launch_pipe<T, RR, true>(si, ns, phased, nlf, grid, nthr, smem, st, x, xold, out, V, G, C, NL, err); \
+        else launch_pipe<T, RR, false>(si, ns, phased, nlf, grid, nthr, smem, st, x, xold, out, V, G, C, NL, err);   \
         break;
     switch (R) {
         LYNX_PIPE_CASE(1)
@@ -229,19 +262,19 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
 #if LYNX_STENCIL_TYPES == 0
 template int launch_cheb_pipe<double, double>(const StencilGeom&, int, const double*, long long, const double*,
                                               long long, double*, long long, const double*, int, double, double,
-                                              double, const double*, const double*, int*, cudaStream_t, int);
+                                              double, const double*, const double*, int*, cudaStream_t, int, const PipeNLHost*);
 template int launch_cheb_pipe<float, float>(const StencilGeom&, int, const float*, long long, const float*,
                                             long long, float*, long long, const float*, int, double, double, double,
-                                            const float*, const float*, int*, cudaStream_t, int);
+                                            const float*, const float*, int*, cudaStream_t, int, const PipeNLHost*);
 template int pipe_shape_count<double>(int);
 template int pipe_shape_count<float>(int);
 #else
 template int launch_cheb_pipe<double2, double>(const StencilGeom&, int, const double2*, long long, const double2*,
                                                long long, double2*, long long, const double*, int, double, double,
-                                               double, const double2*, const double2*, int*, cudaStream_t, int);
+                                               double, const double2*, const double2*, int*, cudaStream_t, int, const PipeNLHost*);
 template int launch_cheb_pipe<float2, float>(const StencilGeom&, int, const float2*, long long, const float2*,
                                              long long, float2*, long long, const float*, int, double, double,
-                                             double, const float2*, const float2*, int*, cudaStream_t, int);
+                                             double, const float2*, const float2*, int*, cudaStream_t, int, const PipeNLHost*);
 template int pipe_shape_count<double2>(int);
 template int pipe_shape_count<float2>(int);
 #endif

@@ -30,7 +30,7 @@ def system(synth_psp8):
     ctx = solver.Context(cl)
     tab = P.nonlocal_tables(cl, pos, P.read_psp8(synth_psp8))
     ctx.set_nonlocal(tab)
-    return dict(cell=cl, pos=pos, V=V, R=R, ctx=ctx, solver=solver, torch=torch)
+    return dict(cell=cl, pos=pos, V=V, R=R, ctx=ctx, solver=solver, torch=torch, synth_psp8=synth_psp8)
 
 
 def test_grid_matches_reference(system):
@@ -243,3 +243,27 @@ def test_mixed_pass_tensor_core_gram(system, nstates):
     assert np.all(np.diff(eigm) >= -1e-9)
     assert np.abs(eigm - eig64).max() < 2e-5
     assert subspace_distance(out["mixed"][0], out["fp64"][0]) < 1e-3
+
+
+def test_fused_nonlocal_and_shapes_bitwise(system):
+    """The fused nonlocal term (stencil kernel adds a * chi alpha) and every launch shape give
+    bitwise the results of the separate-scatter default-shape path (same operations, same order)."""
+    from lynx_b200 import _lib
+    s = system
+    lo, hi, lc = _bounds(s)
+    X = C.random_orbitals(s["ctx"].nd, 20, seed=91)
+    out = {}
+    for fuse in (0, 1):
+        for tune in (0, 1):
+            ctx = s["solver"].Context(s["cell"])
+            ctx.set_nonlocal(P.nonlocal_tables(s["cell"], s["pos"], P.read_psp8(s["synth_psp8"])))
+            _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_FUSE_NONLOCAL, fuse))
+            _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_AUTOTUNE, tune))
+            es = s["solver"].EigenSolver(ctx)
+            for prec in ("fp64", "mixed"):
+                out[(fuse, tune, prec)] = es.chebyshev_filter(X, s["V"], lc, lo, hi, 6, precision=prec)
+            ctx.close()
+    for prec in ("fp64", "mixed"):
+        ref_ = out[(0, 0, prec)]
+        for key in ((0, 1), (1, 0), (1, 1)):
+            assert np.array_equal(out[key + (prec,)], ref_), (key, prec)
