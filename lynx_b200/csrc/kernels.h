@@ -15,6 +15,21 @@ struct StencilGeom {
     const double* D2z;
 };
 
+// Mixed-derivative coefficients of a non-orthogonal cell (host arrays of R+1 values).
+struct NonOrthGeom {
+    int nx, ny, nz, R;
+    const double* D1y;
+    const double* D1z;
+    const double* D2xy;
+    const double* D2xz;
+    const double* D2yz;
+};
+// out += a * (-1/2) * (mixed-derivative part of Lap x); gy, gz: scratch blocks like x (column
+// stride ldg).  nonorth.cu.
+template <typename T>
+int launch_nonorth_terms(const NonOrthGeom& g, int nxp, const T* x, long long ldx, T* gy, T* gz, long long ldg, T* out,
+                         long long ldout, int ncol, double a, const T* phl, const T* phr, cudaStream_t st);
+
 // out = a*(-0.5*Lap x + V.*x) + b*x + d*xold over ncol columns (xold may be null when d == 0).
 // phl/phr: per-direction ghost multipliers (3 values of T each).
 template <typename T, typename S>

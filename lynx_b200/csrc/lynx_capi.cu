@@ -181,6 +181,7 @@ struct lynx_ctx {
     std::map<int, NLMap> nl_maps;  // per padded row length: compact point map of the sphere points
     DevBuf nlW;                    // compact (chi alpha) values, columns of ldw
     DevBuf xsbuf[2];               // compact sphere-point copies of consecutive filter blocks
+    DevBuf gradbuf[2];             // first derivatives along y and z (non-orthogonal cells)
     // nonlocal tables re-indexed for padded row layouts: nxp -> tables
     std::map<int, NLDev> nl_layouts;
     std::vector<DevBuf> nl_layout_bufs;
@@ -611,7 +612,7 @@ int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, lo
     // Fused nonlocal term: real data, periodic cell, pipelined kernel, disjoint spheres.  The
     // values (chi alpha) are expanded to the compact point numbering and added by the stencil
     // kernel itself (out += a * W), in the order the separate scatter would add them.
-    const bool fuse = c->has_nl && c->fuse_nl && pipe_ok && !ScalarOf<T>::cplx && !use_k && c->nl.compact &&
+    const bool fuse = c->has_nl && c->fuse_nl && c->orth && pipe_ok && !ScalarOf<T>::cplx && !use_k && c->nl.compact &&
                       c->nl.n_colors == 1 && geom(c).R == 6 && c->bc[0] == LYNX_BC_PERIODIC &&
                       c->bc[1] == LYNX_BC_PERIODIC && c->bc[2] == LYNX_BC_PERIODIC;
     const long long ldw = ((long long)c->nl.n_pts + 3) & ~3LL;  // compact column stride
@@ -647,6 +648,15 @@ int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, lo
         LYNX_TRY(pipe_launch_tuned<T, S>(c, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, nullptr));
     } else {
         LYNX_TRY(launch_cheb_step<T, S>(geom(c), x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, c->stream));
+    }
+    if (!c->orth) {
+        // mixed-derivative terms of a non-orthogonal cell, from two first-derivative blocks
+        const long long ldg = (long long)nxp * c->ny * c->nz;
+        for (int i = 0; i < 2; ++i) LYNX_TRY(c->gradbuf[i].ensure(sizeof(T) * (size_t)ldg * ncol));
+        NonOrthGeom ng{c->nx, c->ny, c->nz, geom(c).R, c->D1y.data(), c->D1z.data(), c->D2xy.data(), c->D2xz.data(),
+                       c->D2yz.data()};
+        LYNX_TRY(launch_nonorth_terms<T>(ng, nxp, x, ldx, c->gradbuf[0].as<T>(), c->gradbuf[1].as<T>(), ldg, out, ldout,
+                                         ncol, a, phl, phr, c->stream));
     }
     if (c->has_nl)
         LYNX_TRY(launch_nl_scatter<T, S>(*nl, out, ldout, ncol, c->alpha.as<T>(), ncolp, (S)a, c->stream));
@@ -969,10 +979,6 @@ int solve_impl(lynx_ctx* c, T64* psi, double* eig, const double* veff, int N, in
     LYNX_CHECK_ARG(degree >= 1, "cheb_degree must be >= 1");
     LYNX_CHECK_ARG(precision == LYNX_PREC_FP64 || precision == LYNX_PREC_MIXED, "unknown precision");
     LYNX_CHECK_ARG(emax > lc && emin < lc, "spectral bounds must satisfy eigmin < lambda_cutoff < eigmax");
-    if (!c->orth) {
-        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
-        return LYNX_ERR_UNSUPPORTED;
-    }
     LYNX_TRY(activate(c));
     const long long Nd = c->Nd;
     const long long ldp = ld > 0 ? ld : Nd;
@@ -1071,10 +1077,6 @@ int lanczos_impl(lynx_ctx* c, const double* veff, double tol, int max_iter, doub
                  bool use_k) {
     LYNX_CHECK_ARG(c && veff && eigmin && eigmax, "null pointer");
     LYNX_CHECK_ARG(max_iter >= 1, "max_iter must be >= 1");
-    if (!c->orth) {
-        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
-        return LYNX_ERR_UNSUPPORTED;
-    }
     LYNX_TRY(activate(c));
     const bool cplx = sizeof(T) == sizeof(double2);
     const long long Nv = cplx ? 2LL * c->Nd : c->Nd;  // doubles per vector
@@ -1313,6 +1315,8 @@ int lynx_destroy(lynx_ctx* c) {
     c->nlW.release();
     c->xsbuf[0].release();
     c->xsbuf[1].release();
+    c->gradbuf[0].release();
+    c->gradbuf[1].release();
     for (auto& b : c->nl_layout_bufs) b.release();
     for (auto& kv : c->nl_maps) {
         kv.second.ptmap.release();
@@ -1553,10 +1557,6 @@ int lynx_hamiltonian_apply(lynx_ctx* c, const double* psi, const double* veff, d
                            double cs) {
     LYNX_CHECK_ARG(c && psi && veff && y, "null pointer");
     LYNX_CHECK_ARG(ncol >= 0, "negative ncol");
-    if (!c->orth) {
-        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
-        return LYNX_ERR_UNSUPPORTED;
-    }
     LYNX_TRY(activate(c));
     const long long l = ld > 0 ? ld : c->Nd;
     LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
@@ -1570,10 +1570,6 @@ int lynx_hamiltonian_apply_kpt(lynx_ctx* c, const double* psi, const double* vef
                                double cs) {
     LYNX_CHECK_ARG(c && psi && veff && y, "null pointer");
     LYNX_CHECK_ARG(ncol >= 0, "negative ncol");
-    if (!c->orth) {
-        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
-        return LYNX_ERR_UNSUPPORTED;
-    }
     LYNX_TRY(activate(c));
     const long long l = ld > 0 ? ld : c->Nd;
     LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
@@ -1614,10 +1610,6 @@ static int filter_entry(lynx_ctx* c, const double* X, double* Y, const double* v
     LYNX_CHECK_ARG(ncol > 0 && degree >= 1, "ncol and degree must be positive");
     LYNX_CHECK_ARG(precision == LYNX_PREC_FP64 || precision == LYNX_PREC_MIXED, "unknown precision");
     LYNX_CHECK_ARG(emax > lc && emin < lc, "spectral bounds must satisfy eigmin < lambda_cutoff < eigmax");
-    if (!c->orth) {
-        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
-        return LYNX_ERR_UNSUPPORTED;
-    }
     LYNX_TRY(activate(c));
     const long long Nd = c->Nd, l = ld > 0 ? ld : Nd;
     LYNX_CHECK_ARG(l >= Nd, "ld < Nd");
@@ -1705,10 +1697,6 @@ int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precisi
     LYNX_CHECK_ARG(c && veff && ms_per_step, "null pointer");
     LYNX_CHECK_ARG(ncol > 0 && reps > 0, "ncol and reps must be positive");
     LYNX_CHECK_ARG(precision == LYNX_PREC_FP64 || precision == LYNX_PREC_MIXED, "unknown precision");
-    if (!c->orth) {
-        set_error("non-orthogonal cells are not supported by this build's stencil kernel");
-        return LYNX_ERR_UNSUPPORTED;
-    }
     LYNX_TRY(activate(c));
     const size_t esz = precision == LYNX_PREC_FP64 ? sizeof(double) : sizeof(float);
     const int nxp = (c->nx % 2 == 0) ? pipe_row_elems(c->nx, esz) : c->nx;

@@ -1,0 +1,167 @@
+// Mixed-derivative terms of the Laplacian on non-orthogonal cells
+// (src/operators/Hamiltonian.cpp:177-267, lap_plus_diag_nonorth_impl):
+//   Lap += sum_{p,q} c_ab[p] d1_b[q] (x(+pa+qb) - x(+pa-qb) - x(-pa+qb) + x(-pa-qb))
+// for (a,b) = (x,y), (x,z), (y,z), with c_ab = D2_coeff_{xy,xz,yz} and d1_b = D1_coeff_{y,z}.
+// Evaluated in separable form: first the first derivatives along y and z,
+//   gy = sum_q d1_y[q] (x(+qy) - x(-qy)),   gz = sum_q d1_z[q] (x(+qz) - x(-qz)),
+// then  mixed = sum_p c_xy[p] (gy(+px) - gy(-px)) + c_xz[p] (gz(+px) - gz(-px))
+//             + c_yz[p] (gz(+py) - gz(-py)),
+// and out += a * (-1/2) * mixed.  (The same sums in another order: O(R) work per point
+// instead of O(R^2).)  Wrapped neighbours carry the ghost multipliers of the periodic / Bloch /
+// Dirichlet boundary, as in the stencil kernels; gy and gz are Bloch functions with the same
+// multipliers.  Rows have nxp elements (x >= nx is padding and is not written).
+#include "kernels.h"
+#include "lynx_common.cuh"
+#include "stencil.cuh"
+
+namespace lynxb {
+namespace {
+
+template <typename T>
+struct NOArgs {
+    using S = typename ScalarOf<T>::type;
+    int nx, ny, nz, nxp, R;
+    S d1y[9], d1z[9], cxy[9], cxz[9], cyz[9];
+    T phl[3], phr[3];
+};
+
+template <typename T>
+__device__ __forceinline__ T wrapped(const T* base, long long idx, bool l, bool r, const T& phl, const T& phr) {
+    const T v = base[idx];
+    if (l) return pmul(v, phl);
+    if (r) return pmul(v, phr);
+    return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    nonorth_grad_kernel(const T* __restrict__ x, long long ldx, T* __restrict__ gy, T* __restrict__ gz, long long ldg,
+                        const NOArgs<T> A) {
+    const long long np = (long long)A.nx * A.ny * A.nz;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const int col = blockIdx.y;
+    const int i = (int)(t % A.nx);
+    const int j = (int)((t / A.nx) % A.ny);
+    const int k = (int)(t / ((long long)A.nx * A.ny));
+    const T* xb = x + (long long)col * ldx;
+    auto at = [&](int ii, int jj, int kk) { return (long long)ii + (long long)A.nxp * (jj + (long long)A.ny * kk); };
+    T sy = vzero(T()), sz = vzero(T());
+    for (int q = 1; q <= A.R; ++q) {
+        int jp = j + q, jm = j - q;
+        const bool ry = jp >= A.ny, ly = jm < 0;
+        jp -= ry ? A.ny : 0;
+        jm += ly ? A.ny : 0;
+        const T yp = wrapped(xb, at(i, jp, k), false, ry, A.phl[1], A.phr[1]);
+        const T ym = wrapped(xb, at(i, jm, k), ly, false, A.phl[1], A.phr[1]);
+        sy = fmac(sy, A.d1y[q], vadd(yp, vscale((typename ScalarOf<T>::type)(-1), ym)));
+        int kp = k + q, km = k - q;
+        const bool rz = kp >= A.nz, lz = km < 0;
+        kp -= rz ? A.nz : 0;
+        km += lz ? A.nz : 0;
+        const T zp = wrapped(xb, at(i, j, kp), false, rz, A.phl[2], A.phr[2]);
+        const T zm = wrapped(xb, at(i, j, km), lz, false, A.phl[2], A.phr[2]);
+        sz = fmac(sz, A.d1z[q], vadd(zp, vscale((typename ScalarOf<T>::type)(-1), zm)));
+    }
+    const long long o = (long long)col * ldg + at(i, j, k);
+    gy[o] = sy;
+    gz[o] = sz;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    nonorth_mixed_kernel(const T* __restrict__ gy, const T* __restrict__ gz, long long ldg, T* __restrict__ out,
+                         long long ldout, typename ScalarOf<T>::type scale, const NOArgs<T> A) {
+    const long long np = (long long)A.nx * A.ny * A.nz;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const int col = blockIdx.y;
+    const int i = (int)(t % A.nx);
+    const int j = (int)((t / A.nx) % A.ny);
+    const int k = (int)(t / ((long long)A.nx * A.ny));
+    const T* gyb = gy + (long long)col * ldg;
+    const T* gzb = gz + (long long)col * ldg;
+    auto at = [&](int ii, int jj, int kk) { return (long long)ii + (long long)A.nxp * (jj + (long long)A.ny * kk); };
+    using S = typename ScalarOf<T>::type;
+    T m = vzero(T());
+    for (int p = 1; p <= A.R; ++p) {
+        int ip = i + p, im = i - p;
+        const bool rx = ip >= A.nx, lx = im < 0;
+        ip -= rx ? A.nx : 0;
+        im += lx ? A.nx : 0;
+        const T dyx = vadd(wrapped(gyb, at(ip, j, k), false, rx, A.phl[0], A.phr[0]),
+                           vscale(S(-1), wrapped(gyb, at(im, j, k), lx, false, A.phl[0], A.phr[0])));
+        const T dzx = vadd(wrapped(gzb, at(ip, j, k), false, rx, A.phl[0], A.phr[0]),
+                           vscale(S(-1), wrapped(gzb, at(im, j, k), lx, false, A.phl[0], A.phr[0])));
+        int jp = j + p, jm = j - p;
+        const bool ry = jp >= A.ny, ly = jm < 0;
+        jp -= ry ? A.ny : 0;
+        jm += ly ? A.ny : 0;
+        const T dzy = vadd(wrapped(gzb, at(i, jp, k), false, ry, A.phl[1], A.phr[1]),
+                           vscale(S(-1), wrapped(gzb, at(i, jm, k), ly, false, A.phl[1], A.phr[1])));
+        m = fmac(m, A.cxy[p], dyx);
+        m = fmac(m, A.cxz[p], dzx);
+        m = fmac(m, A.cyz[p], dzy);
+    }
+    T* o = out + (long long)col * ldout + at(i, j, k);
+    *o = fmac(*o, scale, m);
+}
+
+}  // namespace
+
+template <typename T>
+int launch_nonorth_terms(const NonOrthGeom& g, int nxp, const T* x, long long ldx, T* gy, T* gz, long long ldg, T* out,
+                         long long ldout, int ncol, double a, const T* phl, const T* phr, cudaStream_t st) {
+    using S = typename ScalarOf<T>::type;
+    if (g.R < 1 || g.R > 8) {
+        set_error("FD half-width %d outside the supported range 1..8", g.R);
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    if (ncol <= 0) return LYNX_OK;
+    if (ncol > 65535) {
+        set_error("too many columns (%d) for one launch", ncol);
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    NOArgs<T> A;
+    A.nx = g.nx;
+    A.ny = g.ny;
+    A.nz = g.nz;
+    A.nxp = nxp;
+    A.R = g.R;
+    for (int p = 0; p <= 8; ++p) {
+        const bool in = p <= g.R;
+        A.d1y[p] = in ? (S)g.D1y[p] : S(0);
+        A.d1z[p] = in ? (S)g.D1z[p] : S(0);
+        A.cxy[p] = in ? (S)g.D2xy[p] : S(0);
+        A.cxz[p] = in ? (S)g.D2xz[p] : S(0);
+        A.cyz[p] = in ? (S)g.D2yz[p] : S(0);
+    }
+    for (int d = 0; d < 3; ++d) {
+        A.phl[d] = phl[d];
+        A.phr[d] = phr[d];
+    }
+    const long long np = (long long)g.nx * g.ny * g.nz;
+    dim3 grid((unsigned)((np + 255) / 256), ncol);
+    nonorth_grad_kernel<T><<<grid, 256, 0, st>>>(x, ldx, gy, gz, ldg, A);
+    nonorth_mixed_kernel<T><<<grid, 256, 0, st>>>(gy, gz, ldg, out, ldout, (S)(-0.5 * a), A);
+    count_launch(2);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("non-orthogonal stencil launch failed: %s", cudaGetErrorString(e));
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+template int launch_nonorth_terms<double>(const NonOrthGeom&, int, const double*, long long, double*, double*, long long,
+                                          double*, long long, int, double, const double*, const double*, cudaStream_t);
+template int launch_nonorth_terms<float>(const NonOrthGeom&, int, const float*, long long, float*, float*, long long,
+                                         float*, long long, int, double, const float*, const float*, cudaStream_t);
+template int launch_nonorth_terms<double2>(const NonOrthGeom&, int, const double2*, long long, double2*, double2*,
+                                           long long, double2*, long long, int, double, const double2*, const double2*,
+                                           cudaStream_t);
+template int launch_nonorth_terms<float2>(const NonOrthGeom&, int, const float2*, long long, float2*, float2*,
+                                          long long, float2*, long long, int, double, const float2*, const float2*,
+                                          cudaStream_t);
+
+}  // namespace lynxb
