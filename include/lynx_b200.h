@@ -165,6 +165,22 @@ LYNX_API int lynx_lanczos_bounds(lynx_ctx* ctx, const double* veff, double tol, 
 LYNX_API int lynx_lanczos_bounds_kpt(lynx_ctx* ctx, const double* veff, double tol, int max_iter, double* eigmin,
                             double* eigmax);
 
+/* Nonlocal forces and energy of device orbitals psi (nband columns, column stride ld; real):
+ *   force[3a + d] = -2 occfac sum_n occ[n] sum_p Gamma_p alpha_{p,n} beta_{p,n,d},
+ *   *energy_nl    =    occfac sum_n occ[n] sum_p Gamma_p alpha_{p,n}^2,
+ * alpha = dV chi^T psi summed over the atom's images, beta_d the same projection of the FD first
+ * derivative of psi along lattice direction d.  occ: host, nband occupations; force: host,
+ * 3 * n_atom doubles; energy_nl may be NULL.  Replaces Hamiltonian::compute_nonlocal_force_gpu
+ * (src/operators/Hamiltonian.hpp:150-153; the formula of src/physics/Forces.cpp:509-797). */
+LYNX_API int lynx_nonlocal_force(lynx_ctx* ctx, const double* psi, int nband, int ld, const double* occ, double occfac,
+                                 double* force, double* energy_nl);
+/* Complex k-point version at the context's k-point: force = -spn_fac_wk sum_n occ sum_p Gamma
+ * Re(conj(alpha) beta), energy = (spn_fac_wk / 2) sum_n occ sum_p Gamma |alpha|^2, with the Bloch
+ * factors of the nonlocal apply.  Replaces Hamiltonian::compute_nonlocal_force_kpt_gpu
+ * (src/operators/Hamiltonian.hpp:163-166). */
+LYNX_API int lynx_nonlocal_force_kpt(lynx_ctx* ctx, const double* psi_z, int nband, int ld, const double* occ,
+                                     double spn_fac_wk, double* force, double* energy_nl);
+
 /* Fermi level by Brent's method on sum_i w_i f(eps_i - Ef) = nelectron (tolerance 1e-14, <= 200
  * iterations), f Fermi-Dirac or Gaussian smearing.  Host arrays, FP64.
  * Replaces Occupation::find_fermi_level (src/electronic/Occupation.cpp:48-84). */

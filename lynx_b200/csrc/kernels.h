@@ -147,6 +147,15 @@ int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alp
 template <typename T, typename S>
 int launch_nl_scatter(const NLDev& nl, T* out, long long ld, int ncol, const T* alpha, int ncolp, S scale,
                       cudaStream_t st);
+// Nonlocal force of one direction and per-atom energy from projections without Gamma (alpha of
+// psi, beta of its derivative), occupations occ (device): see nonlocal.cuh.
+template <typename T>
+int launch_nl_force_reduce(const NLDev& nl, const T* alpha, const T* beta, int ncolp, int ncol, const double* occ,
+                           double spn, double efac, int dim, double* force, double* ea, cudaStream_t st);
+// First derivative along lattice direction dir (D1: R+1 host coefficients); nonorth.cu.
+template <typename T>
+int launch_grad_dir(int nx, int ny, int nz, int nxp, int R, const double* D1, int dir, const T* x, long long ldx,
+                    T* g, long long ldg, int ncol, const T* phl, const T* phr, cudaStream_t st);
 // W[col * ldw + point] = (chi alpha)(point, col) on the compact point numbering (nl.compact).
 template <typename T>
 int launch_nl_expand(const NLDev& nl, T* W, long long ldw, int ncol, const T* alpha, int ncolp, cudaStream_t st);

@@ -182,6 +182,7 @@ struct lynx_ctx {
     DevBuf nlW;                    // compact (chi alpha) values, columns of ldw
     DevBuf xsbuf[2];               // compact sphere-point copies of consecutive filter blocks
     DevBuf gradbuf[2];             // first derivatives along y and z (non-orthogonal cells)
+    DevBuf fbeta, fwork, fones;    // nonlocal forces: derivative projections, occupations/results, ones
     // nonlocal tables re-indexed for padded row layouts: nxp -> tables
     std::map<int, NLDev> nl_layouts;
     std::vector<DevBuf> nl_layout_bufs;
@@ -1317,6 +1318,9 @@ int lynx_destroy(lynx_ctx* c) {
     c->xsbuf[1].release();
     c->gradbuf[0].release();
     c->gradbuf[1].release();
+    c->fbeta.release();
+    c->fwork.release();
+    c->fones.release();
     for (auto& b : c->nl_layout_bufs) b.release();
     for (auto& kv : c->nl_maps) {
         kv.second.ptmap.release();
@@ -1822,6 +1826,72 @@ int noalloc_scratch(int device, void** out) {
     return LYNX_OK;
 }
 }  // namespace
+
+// Nonlocal forces (src/physics/Forces.cpp:509-797): projections without Gamma of psi and of its
+// FD derivative along each lattice direction, reduced per atom with the occupations.
+template <typename T>
+int nonlocal_force_impl(lynx_ctx* c, const T* psi, int nband, int ld, const double* occ, double spn, double efac,
+                        double* force, double* energy, bool use_k) {
+    LYNX_CHECK_ARG(c && psi && occ && force, "null pointer");
+    LYNX_CHECK_ARG(nband > 0, "nband must be positive");
+    const long long l = ld > 0 ? ld : c->Nd;
+    LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
+    if (!c->has_nl) {
+        if (energy) *energy = 0.0;
+        return LYNX_OK;
+    }
+    LYNX_TRY(activate(c));
+    const int na = c->nl.n_atom;
+    const int ncolp = ((nband + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
+    const size_t ab = sizeof(T) * (size_t)c->nl.total_proj * ncolp;
+    LYNX_TRY(c->alpha.ensure(ab));
+    LYNX_TRY(c->fbeta.ensure(ab));
+    LYNX_TRY(c->gradbuf[0].ensure(sizeof(T) * (size_t)c->Nd * nband));
+    LYNX_TRY(c->fwork.ensure(sizeof(double) * ((size_t)nband + 4 * (size_t)na)));
+    const std::vector<double> ones(c->nl.total_proj, 1.0);
+    LYNX_TRY(c->fones.ensure(sizeof(double) * ones.size()));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(c->fones.p, ones.data(), sizeof(double) * ones.size(), cudaMemcpyHostToDevice,
+                                  c->stream));
+    double* docc = c->fwork.as<double>();
+    double* dforce = docc + nband;
+    double* dea = dforce + 3 * na;
+    LYNX_CUDA_TRY(cudaMemcpyAsync(docc, occ, sizeof(double) * nband, cudaMemcpyHostToDevice, c->stream));
+    NLDev raw = c->nl;  // projections without Gamma
+    raw.gamma = c->fones.as<double>();
+    T phl[3], phr[3];
+    ghost_phases<T>(c, use_k, phl, phr);
+    T* g = c->gradbuf[0].as<T>();
+    LYNX_TRY(launch_nl_gather<T>(raw, psi, l, nband, c->alpha.as<T>(), ncolp, c->dV, c->stream));
+    const double* D1[3] = {c->D1x.data(), c->D1y.data(), c->D1z.data()};
+    for (int d = 0; d < 3; ++d) {
+        LYNX_TRY(launch_grad_dir<T>(c->nx, c->ny, c->nz, c->nx, geom(c).R, D1[d], d, psi, l, g, c->Nd, nband, phl, phr,
+                                    c->stream));
+        LYNX_TRY(launch_nl_gather<T>(raw, g, c->Nd, nband, c->fbeta.as<T>(), ncolp, c->dV, c->stream));
+        LYNX_TRY(launch_nl_force_reduce<T>(c->nl, c->alpha.as<T>(), c->fbeta.as<T>(), ncolp, nband, docc, spn, efac, d,
+                                           dforce, dea, c->stream));
+    }
+    std::vector<double> ea(na);
+    LYNX_CUDA_TRY(cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, c->stream));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(ea.data(), dea, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (energy) {
+        double e = 0.0;
+        for (int a = 0; a < na; ++a) e += ea[a];
+        *energy = e;
+    }
+    return LYNX_OK;
+}
+
+extern "C" int lynx_nonlocal_force(lynx_ctx* c, const double* psi, int nband, int ld, const double* occ, double occfac,
+                                   double* force, double* energy_nl) {
+    return nonlocal_force_impl<double>(c, psi, nband, ld, occ, 2.0 * occfac, occfac, force, energy_nl, false);
+}
+
+extern "C" int lynx_nonlocal_force_kpt(lynx_ctx* c, const double* psi_z, int nband, int ld, const double* occ,
+                                       double spn_fac_wk, double* force, double* energy_nl) {
+    return nonlocal_force_impl<double2>(c, reinterpret_cast<const double2*>(psi_z), nband, ld, occ, spn_fac_wk,
+                                        0.5 * spn_fac_wk, force, energy_nl, true);
+}
 
 extern "C" int lynx_set_option(lynx_ctx* c, int option, int value) {
     LYNX_CHECK_ARG(c != nullptr, "null context");

@@ -558,4 +558,44 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// Nonlocal force reduction for one direction (src/physics/Forces.cpp:772-777, :682-684):
+//   force[a * 3 + dim] = -spn * sum_n occ[n] sum_{j < np(a)} Gamma[poff+j] Re(conj(alpha) beta)
+// and, for dim == 0, the atom's energy share  ea[a] = efac * sum_n occ[n] sum_j Gamma |alpha|^2.
+// alpha, beta: projections without Gamma, [total_proj][ncolp].  CTA = atom; fixed-order sums.
+__device__ __forceinline__ double re_conj_mul(double a, double b) { return a * b; }
+__device__ __forceinline__ double re_conj_mul(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    nl_force_reduce_kernel(const T* __restrict__ alpha, const T* __restrict__ beta, int ncolp, int ncol,
+                           const double* __restrict__ occ, const int* __restrict__ atom_nproj,
+                           const int* __restrict__ atom_poff, const double* __restrict__ gamma, double spn,
+                           double efac, int dim, double* __restrict__ force, double* __restrict__ ea) {
+    __shared__ double rf[256], re[256];
+    const int a = blockIdx.x;
+    const int np = atom_nproj[a], poff = atom_poff[a];
+    double sf = 0.0, se = 0.0;
+    for (int e = threadIdx.x; e < np * ncol; e += blockDim.x) {
+        const int j = e / ncol, n = e % ncol;
+        const long long o = (long long)(poff + j) * ncolp + n;
+        const double w = occ[n] * gamma[poff + j];
+        sf += w * re_conj_mul(alpha[o], beta[o]);
+        if (dim == 0) se += w * re_conj_mul(alpha[o], alpha[o]);
+    }
+    rf[threadIdx.x] = sf;
+    re[threadIdx.x] = se;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) {
+            rf[threadIdx.x] += rf[threadIdx.x + h];
+            re[threadIdx.x] += re[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        force[a * 3 + dim] = -spn * rf[0];
+        if (dim == 0) ea[a] = efac * re[0];
+    }
+}
+
 }  // namespace lynxb

@@ -156,6 +156,20 @@ int launch_nl_expand(const NLDev& nl, T* W, long long ldw, int ncol, const T* al
     }
 }
 
+template <typename T>
+int launch_nl_force_reduce(const NLDev& nl, const T* alpha, const T* beta, int ncolp, int ncol, const double* occ,
+                           double spn, double efac, int dim, double* force, double* ea, cudaStream_t st) {
+    if (nl.n_atom == 0 || ncol <= 0) return LYNX_OK;
+    nl_force_reduce_kernel<T><<<nl.n_atom, 256, 0, st>>>(alpha, beta, ncolp, ncol, occ, nl.atom_nproj, nl.atom_poff,
+                                                         nl.gamma, spn, efac, dim, force, ea);
+    count_launch();
+    return launch_status("nonlocal force reduction");
+}
+template int launch_nl_force_reduce<double>(const NLDev&, const double*, const double*, int, int, const double*, double,
+                                            double, int, double*, double*, cudaStream_t);
+template int launch_nl_force_reduce<double2>(const NLDev&, const double2*, const double2*, int, int, const double*,
+                                             double, double, int, double*, double*, cudaStream_t);
+
 template int launch_nl_expand<double>(const NLDev&, double*, long long, int, const double*, int, cudaStream_t);
 template int launch_nl_expand<float>(const NLDev&, float*, long long, int, const float*, int, cudaStream_t);
 template int launch_nl_gather<double>(const NLDev&, const double*, long long, int, double*, int, double, cudaStream_t);

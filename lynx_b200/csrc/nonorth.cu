@@ -165,3 +165,91 @@ template int launch_nonorth_terms<float2>(const NonOrthGeom&, int, const float2*
                                           cudaStream_t);
 
 }  // namespace lynxb
+
+// ---------------------------------------------------------------------------------------------
+// First derivative along one lattice direction (src/operators/Gradient.cpp:17-62):
+//   g = sum_p D1[p] (x(+p e_dir) - x(-p e_dir)), ghosts as in the stencil kernels.
+// ---------------------------------------------------------------------------------------------
+namespace lynxb {
+namespace {
+template <typename T>
+struct GradArgs {
+    using S = typename ScalarOf<T>::type;
+    int nx, ny, nz, nxp, R, dir;
+    S d1[9];
+    T phl, phr;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+    grad_dir_kernel(const T* __restrict__ x, long long ldx, T* __restrict__ g, long long ldg, const GradArgs<T> A) {
+    const long long np = (long long)A.nx * A.ny * A.nz;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= np) return;
+    const int col = blockIdx.y;
+    const int c[3] = {(int)(t % A.nx), (int)((t / A.nx) % A.ny), (int)(t / ((long long)A.nx * A.ny))};
+    const int n[3] = {A.nx, A.ny, A.nz};
+    const T* xb = x + (long long)col * ldx;
+    auto at = [&](const int* q) { return (long long)q[0] + (long long)A.nxp * (q[1] + (long long)A.ny * q[2]); };
+    using S = typename ScalarOf<T>::type;
+    T s = vzero(T());
+    const int d = A.dir;
+    for (int p = 1; p <= A.R; ++p) {
+        int q[3] = {c[0], c[1], c[2]};
+        int ip = c[d] + p, im = c[d] - p;
+        const bool r = ip >= n[d], l = im < 0;
+        ip -= r ? n[d] : 0;
+        im += l ? n[d] : 0;
+        q[d] = ip;
+        T vp = xb[at(q)];
+        if (r) vp = pmul(vp, A.phr);
+        q[d] = im;
+        T vm = xb[at(q)];
+        if (l) vm = pmul(vm, A.phl);
+        s = fmac(s, A.d1[p], vadd(vp, vscale(S(-1), vm)));
+    }
+    g[(long long)col * ldg + at(c)] = s;
+}
+}  // namespace
+
+template <typename T>
+int launch_grad_dir(int nx, int ny, int nz, int nxp, int R, const double* D1, int dir, const T* x, long long ldx,
+                    T* g, long long ldg, int ncol, const T* phl, const T* phr, cudaStream_t st) {
+    using S = typename ScalarOf<T>::type;
+    if (R < 1 || R > 8 || dir < 0 || dir > 2) {
+        set_error("gradient: bad half-width %d or direction %d", R, dir);
+        return LYNX_ERR_BAD_ARG;
+    }
+    if (ncol <= 0) return LYNX_OK;
+    if (ncol > 65535) {
+        set_error("too many columns (%d) for one launch", ncol);
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    GradArgs<T> A;
+    A.nx = nx;
+    A.ny = ny;
+    A.nz = nz;
+    A.nxp = nxp;
+    A.R = R;
+    A.dir = dir;
+    for (int p = 0; p <= 8; ++p) A.d1[p] = (p <= R) ? (S)D1[p] : S(0);
+    A.phl = phl[dir];
+    A.phr = phr[dir];
+    const long long np = (long long)nx * ny * nz;
+    dim3 grid((unsigned)((np + 255) / 256), ncol);
+    grad_dir_kernel<T><<<grid, 256, 0, st>>>(x, ldx, g, ldg, A);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("gradient launch failed: %s", cudaGetErrorString(e));
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+template int launch_grad_dir<double>(int, int, int, int, int, const double*, int, const double*, long long, double*,
+                                     long long, int, const double*, const double*, cudaStream_t);
+template int launch_grad_dir<double2>(int, int, int, int, int, const double*, int, const double2*, long long, double2*,
+                                      long long, int, const double2*, const double2*, cudaStream_t);
+
+}  // namespace lynxb

@@ -119,6 +119,7 @@ class Context:
         check(self.lib.lynx_set_nonlocal(self._h, tab.n_img, iptr(a), iptr(n), dptr(s), iptr(g), dptr(c),
                                          tab.n_atom, iptr(npj), dptr(gm)))
         self.has_nonlocal = True
+        self.n_atom = int(tab.n_atom)
 
     def set_kpoint(self, kcart):
         k = np.ascontiguousarray(kcart, dtype=np.float64).reshape(3)
@@ -190,6 +191,27 @@ class NonlocalProjector:
         fn = ctx.lib.lynx_nonlocal_apply_kpt if kpt else ctx.lib.lynx_nonlocal_apply
         check(fn(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), ctypes.c_void_p(_dev_ptr(h.t)), a.ncol, ctx.nd))
         return h.out(h.t)
+
+    def force(self, psi, occ, occfac: float = 2.0, kpt: bool = False, wk: float = 1.0):
+        """Nonlocal forces (n_atom x 3, Ha/Bohr along the lattice directions) and energy of the
+        orbitals psi with occupations occ (Hamiltonian::compute_nonlocal_force_gpu /
+        _kpt_gpu; the formula of Forces.cpp:509-797).  k-point: spn_fac * wk = 2 occfac wk."""
+        ctx = self.ctx
+        ctx.sync_stream()
+        a = _DeviceArgs(ctx, psi, kpt)
+        occ = np.ascontiguousarray(occ, dtype=np.float64)
+        if occ.shape[0] != a.ncol:
+            raise ValueError("one occupation per orbital column is needed")
+        na = getattr(ctx, "n_atom", 0)
+        f = np.zeros(3 * max(na, 1))
+        e = np.zeros(1)
+        if kpt:
+            check(ctx.lib.lynx_nonlocal_force_kpt(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), a.ncol, ctx.nd,
+                                                  dptr(occ), 2.0 * occfac * wk, dptr(f), dptr(e)))
+        else:
+            check(ctx.lib.lynx_nonlocal_force(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), a.ncol, ctx.nd, dptr(occ),
+                                              occfac * wk, dptr(f), dptr(e)))
+        return f[:3 * na].reshape(na, 3), float(e[0])
 
 
 class Hamiltonian:

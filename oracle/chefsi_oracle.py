@@ -389,3 +389,68 @@ def kpoints(lengths, kgrid, shift=(0.0, 0.0, 0.0)):
                     kr.append(red)
                     w.append(1.0)
     return np.array(kc), np.array(kr), np.array(w)
+
+
+# ---------------------------------------------------------------------------
+# Nonlocal force and energy (src/physics/Forces.cpp:509-797 compute_nonlocal_cpu,
+# src/operators/Gradient.cpp:17-62; energy as documented at src/physics/GPUForce.cu:168-170)
+# ---------------------------------------------------------------------------
+
+def gradient(psi, shape, st, dim, kpt=None, lengths=None, bc=(0, 0, 0)):
+    """D psi along lattice direction dim: sum_p D1[p] (x(+p) - x(-p)) on the ghost-extended
+    block (Gradient.cpp:17-62; ghosts as HaloExchange::execute / execute_kpt)."""
+    nx, ny, nz = shape
+    c = st["D1" + "xyz"[dim]]
+    fdn = len(c) - 1
+    ph = bloch_phases(kpt, lengths) if kpt is not None else None
+    psi2 = psi.reshape(psi.shape[0], -1)
+    out = np.zeros_like(psi2)
+    for n in range(psi2.shape[1]):
+        xe = extend(psi2[:, n].reshape(nz, ny, nx), fdn, ph, bc)
+
+        def sh(d):
+            off = [0, 0, 0]
+            off[2 - dim] = d  # arrays are (z, y, x)
+            return xe[fdn + off[0]:fdn + off[0] + nz, fdn + off[1]:fdn + off[1] + ny, fdn + off[2]:fdn + off[2] + nx]
+
+        g = np.zeros((nz, ny, nx), dtype=xe.dtype)
+        for p in range(1, fdn + 1):
+            g = g + c[p] * (sh(p) - sh(-p))
+        out[:, n] = g.ravel()
+    return out.reshape(psi.shape)
+
+
+def projections(psi, tab: dict, dV: float, kpt=None):
+    """alpha[atom, jp, n] = dV sum_img e^{-i k.R_img} chi_img^T psi (no Gamma), summed over the
+    images of each atom in image order (Forces.cpp:701-722 real, :598-624 k-point)."""
+    psi2 = psi.reshape(psi.shape[0], -1)
+    nproj = int(tab["nproj"])
+    n_atom = len(tab["gamma"]) // nproj if nproj else 0
+    alpha = np.zeros((n_atom, nproj, psi2.shape[1]), dtype=np.result_type(psi2, 1.0))
+    offs = np.concatenate([[0], np.cumsum(tab["img_ndc"])])
+    for i in range(len(tab["img_atom"])):
+        ndc = int(tab["img_ndc"][i])
+        chi = np.asarray(tab["chi"][offs[i] * nproj:(offs[i] + ndc) * nproj]).reshape(nproj, ndc).T
+        g = tab["gpos"][offs[i]:offs[i] + ndc]
+        fac = dV
+        if kpt is not None:
+            th = -float(np.dot(kpt, tab["img_shift"][i]))
+            fac = complex(math.cos(th), math.sin(th)) * dV
+        alpha[tab["img_atom"][i]] += fac * (chi.T @ psi2[g, :])
+    return alpha
+
+
+def nonlocal_force(psi, occ, tab: dict, st, shape, dV, occfac=2.0, wk=1.0, kpt=None, lengths=None):
+    """Nonlocal forces f[atom, dim] = -spn_fac wk sum_n g_n sum_jp Gamma Re(conj(alpha) beta_dim),
+    spn_fac = 2 occfac, beta_dim = projections of D_dim psi (Forces.cpp:726-778, :662-684), and
+    the nonlocal energy E = occfac wk sum_n g_n sum_jp Gamma |alpha|^2."""
+    nproj = int(tab["nproj"])
+    gam = np.asarray(tab["gamma"]).reshape(-1, nproj)[:, :, None]
+    occ = np.asarray(occ, dtype=np.float64)[None, None, :]
+    alpha = projections(psi, tab, dV, kpt)
+    energy = occfac * wk * float(np.sum(occ * gam * np.abs(alpha) ** 2))
+    f = np.zeros((alpha.shape[0], 3))
+    for dim in range(3):
+        beta = projections(gradient(psi, shape, st, dim, kpt, lengths), tab, dV, kpt)
+        f[:, dim] = -2.0 * occfac * wk * np.sum(occ * gam * np.real(np.conj(alpha) * beta), axis=(1, 2))
+    return f, energy
