@@ -1,0 +1,92 @@
+"""Differentiable operators for PyTorch (torch.autograd.Function), on top of the C ABI.
+
+* ``hamiltonian_apply(ctx, psi, veff)``: y = H psi with H = -0.5 Lap + Veff + Vnl (real, Gamma
+  point).  H is symmetric on the grid (symmetric FD stencil, diagonal Veff, Vnl = dV chi Gamma
+  chi^T), so the adjoint with respect to the orbitals is H itself, grad_psi = H grad_y, and with
+  respect to the potential grad_Veff = sum_n grad_y_n * psi_n.
+* ``nonlocal_energy(ctx, psi, positions, occ, occfac)``: E_nl = occfac sum_n f_n sum_p Gamma_p
+  alpha_{p,n}^2 (alpha = dV chi^T psi_n); grad_psi_n = 2 occfac f_n dV (Vnl psi_n) (d alpha / d psi
+  = dV chi, and Vnl psi = chi Gamma alpha), and grad_positions = -F with F the nonlocal forces of
+  lynx_nonlocal_force (the formula of the reference's Forces::compute_nonlocal,
+  src/physics/Forces.cpp:509-797).  The projector tables of the context must belong to
+  ``positions``; the position gradient is along the lattice directions (Cartesian for orthogonal
+  cells).
+
+Orbitals are torch CUDA tensors of shape (ncol, Nd), float64 (the layout lynx_b200.solver takes
+without copies); the computation runs in liblynxb200.so.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _make_fns():
+    torch = _torch()
+    from . import solver
+
+    class HamiltonianApply(torch.autograd.Function):
+        @staticmethod
+        def forward(fctx, psi, veff, ctx):
+            fctx.ctx = ctx
+            fctx.save_for_backward(psi, veff)
+            return solver.Hamiltonian(ctx).apply(psi.contiguous(), Veff=veff.contiguous())
+
+        @staticmethod
+        def backward(fctx, grad_y):
+            psi, veff = fctx.saved_tensors
+            g = grad_y.contiguous()
+            grad_psi = solver.Hamiltonian(fctx.ctx).apply(g, Veff=veff.contiguous()) if fctx.needs_input_grad[0] else None
+            grad_v = (g * psi).sum(0) if fctx.needs_input_grad[1] else None
+            return grad_psi, grad_v, None
+
+    class NonlocalEnergy(torch.autograd.Function):
+        @staticmethod
+        def forward(fctx, psi, positions, ctx, occ, occfac):
+            occ = np.asarray(occ, dtype=np.float64)
+            f, e = solver.NonlocalProjector(ctx).force(psi.contiguous(), occ, occfac=occfac)
+            fctx.ctx = ctx
+            fctx.occ = occ
+            fctx.occfac = occfac
+            fctx.save_for_backward(psi)
+            fctx.force = torch.as_tensor(f, dtype=positions.dtype, device=positions.device)
+            return torch.tensor(e, dtype=psi.dtype, device=psi.device)
+
+        @staticmethod
+        def backward(fctx, grad_e):
+            (psi,) = fctx.saved_tensors
+            grad_psi = grad_pos = None
+            if fctx.needs_input_grad[0]:
+                vnl = solver.NonlocalProjector(fctx.ctx).apply(psi.contiguous(), torch.zeros_like(psi))
+                w = torch.as_tensor(2.0 * fctx.occfac * fctx.ctx.dV * fctx.occ, dtype=psi.dtype,
+                                    device=psi.device)[:, None]
+                grad_psi = grad_e * w * vnl
+            if fctx.needs_input_grad[1]:
+                grad_pos = -grad_e.to(device=fctx.force.device, dtype=fctx.force.dtype) * fctx.force
+            return grad_psi, grad_pos, None, None, None
+
+    return HamiltonianApply, NonlocalEnergy
+
+
+_FNS = None
+
+
+def _fns():
+    global _FNS
+    if _FNS is None:
+        _FNS = _make_fns()
+    return _FNS
+
+
+def hamiltonian_apply(ctx, psi, veff):
+    """y = H psi, differentiable in psi and veff (see the module docstring)."""
+    return _fns()[0].apply(psi, veff, ctx)
+
+
+def nonlocal_energy(ctx, psi, positions, occ, occfac: float = 2.0):
+    """E_nl of the orbitals psi, differentiable in psi and in the atom positions."""
+    return _fns()[1].apply(psi, positions, ctx, occ, occfac)
