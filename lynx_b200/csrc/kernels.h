@@ -104,6 +104,7 @@ namespace lynxb {
 
 // Device copy of the nonlocal projector tables (see nonlocal.cuh for the layout).
 constexpr int kNLMaxColors = 16;  // colour classes the register-tiled scatter accepts
+constexpr int kNLTilePts = 64;    // points per tile of the register-tiled nonlocal kernels
 
 struct NLDev {
     int n_atom = 0, n_img = 0, n_pts = 0, max_np = 0, total_proj = 0;
@@ -112,6 +113,9 @@ struct NLDev {
     int n_colors = 0;
     int color_off[kNLMaxColors + 1] = {};
     int* color_img = nullptr;
+    // (image, first point) of every 64-point tile, colour class k at color_toff[k] .. [k+1]
+    int color_toff[kNLMaxColors + 1] = {};
+    int2* color_tiles = nullptr;
     // Compact per-point form (only when no grid point lies in two spheres): the distinct
     // points numbered in grid order, ent_pt[entry] = point number of every (image, point) entry.
     bool compact = false;

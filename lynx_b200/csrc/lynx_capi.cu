@@ -1483,7 +1483,7 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
         *dst = b.p;
         return LYNX_OK;
     };
-    c->nl_bufs.reserve(32);
+    c->nl_bufs.reserve(36);
     NLDev& d = c->nl;
     d.n_atom = n_atom;
     d.n_img = n_img;
@@ -1542,6 +1542,17 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
             d.color_off[k + 1] = o;
         }
         LYNX_TRY(up(color_img.data(), color_img.size() * 4, (void**)&d.color_img));
+        std::vector<int> tiles;  // (image, first point) pairs, colour by colour
+        for (int k = 0; k < n_colors; ++k) {
+            d.color_toff[k] = (int)(tiles.size() / 2);
+            for (int q = d.color_off[k]; q < d.color_off[k + 1]; ++q)
+                for (int g0 = 0; g0 < img_ndc[color_img[q]]; g0 += kNLTilePts) {
+                    tiles.push_back(color_img[q]);
+                    tiles.push_back(g0);
+                }
+            d.color_toff[k + 1] = (int)(tiles.size() / 2);
+        }
+        LYNX_TRY(up(tiles.data(), tiles.size() * 4, (void**)&d.color_tiles));
     }
     c->img_shift.assign(img_shift, img_shift + 3 * n_img);
     c->h_gpos.assign(gpos, gpos + tot);

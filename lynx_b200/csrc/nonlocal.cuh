@@ -15,6 +15,7 @@
 // of NB) so that the inner loops need no column guards.
 #pragma once
 #include <cuda_runtime.h>
+#include "kernels.h"
 #include "stencil.cuh"
 
 namespace lynxb {
@@ -207,7 +208,7 @@ __global__ void __launch_bounds__(128)
 // alpha block [projector][column] is read as broadcasts.
 // ---------------------------------------------------------------------------------------------
 constexpr int kNL2Cols = 64;  // columns per CTA of gather2 / scatter2
-constexpr int kNL2Pts = 64;   // points per staged tile
+constexpr int kNL2Pts = kNLTilePts;  // points per staged tile
 
 template <typename T>
 __device__ __forceinline__ void load_vec4(const T* p, T (&v)[4]) {
@@ -421,10 +422,13 @@ template <typename T, bool COMPACT = false>
 __global__ void __launch_bounds__(256)
     nl_scatter2_kernel(T* __restrict__ out, long long ld, int ncol, int ncolp, NLView tab,
                        const int* __restrict__ imgs, const T* __restrict__ alpha, T scale,
-                       const int* __restrict__ ent_pt = nullptr) {
+                       const int* __restrict__ ent_pt = nullptr, const int2* __restrict__ tiles = nullptr) {
     constexpr int NB = kNL2Cols, G = kNL2Pts;
     extern __shared__ __align__(16) unsigned char smraw[];
-    const int im = imgs[blockIdx.x];
+    // tiles (optional): one CTA per (image, first point of a 64-point tile), so the read-modify-
+    // write latencies of all tiles of a colour class overlap; otherwise one CTA per image.
+    const int2 tl = tiles ? tiles[blockIdx.x] : make_int2(imgs[blockIdx.x], 0);
+    const int im = tl.x;
     const int n0 = blockIdx.y * NB;
     const int a = tab.img_atom[im];
     const int np = tab.atom_nproj[a];
@@ -439,7 +443,8 @@ __global__ void __launch_bounds__(256)
         const int j = e / NB, c = e % NB;
         al[e] = (n0 + c < ncolp) ? alpha[(long long)(poff + j) * ncolp + n0 + c] : T(0);
     }
-    for (int g0 = 0; g0 < ndc; g0 += G) {
+    const int gend = tiles ? min(ndc, tl.y + G) : ndc;
+    for (int g0 = tl.y; g0 < gend; g0 += G) {
         __syncthreads();
         for (int e = tid; e < np * G; e += 256) {
             const int j = e / G, g = e % G;

@@ -113,11 +113,11 @@ int launch_nl_scatter(const NLDev& nl, T* out, long long ld, int ncol, const T* 
         if (nl.n_colors > 0 && nl.max_np <= 32) {
             const size_t smem = sizeof(T) * 2 * (size_t)nl.max_np * kNL2Cols;
             for (int k = 0; k < nl.n_colors; ++k) {
-                const int cnt = nl.color_off[k + 1] - nl.color_off[k];
+                const int cnt = nl.color_toff[k + 1] - nl.color_toff[k];
                 if (cnt == 0) continue;
                 dim3 grid(cnt, (ncol + kNL2Cols - 1) / kNL2Cols);
-                nl_scatter2_kernel<T><<<grid, 256, smem, st>>>(out, ld, ncol, ncolp, make_view<T>(nl),
-                                                               nl.color_img + nl.color_off[k], alpha, (T)scale);
+                nl_scatter2_kernel<T><<<grid, 256, smem, st>>>(out, ld, ncol, ncolp, make_view<T>(nl), nullptr, alpha,
+                                                               (T)scale, nullptr, nl.color_tiles + nl.color_toff[k]);
                 count_launch();
                 LYNX_TRY(launch_status("nonlocal scatter"));
             }
