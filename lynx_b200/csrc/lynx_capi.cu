@@ -183,6 +183,10 @@ struct lynx_ctx {
     DevBuf xsbuf[2];               // compact sphere-point copies of consecutive filter blocks
     DevBuf gradbuf[2];             // first derivatives along y and z (non-orthogonal cells)
     DevBuf fbeta, fwork, fones;    // nonlocal forces: derivative projections, occupations/results, ones
+    // Host-input pipelining: a copy stream, and for the duration of one host-pointer solve the
+    // first column of every column block with the event that marks its arrival on the device.
+    cudaStream_t copy_stream = nullptr;
+    std::vector<std::pair<int, cudaEvent_t>> col_blocks;
     // nonlocal tables re-indexed for padded row layouts: nxp -> tables
     std::map<int, NLDev> nl_layouts;
     std::vector<DevBuf> nl_layout_bufs;
@@ -765,13 +769,28 @@ int run_filter32(lynx_ctx* c, const T64* X, long long ldX, const double* veff, i
     const S* Vp = nullptr;
     LYNX_TRY(veff_layout<S>(c, veff, *nxp, &Vp));
     T32* X32 = c->wbuf[3].as<T32>();
-    LYNX_TRY(repack<T32, T64>(c, X32, *nxp, *ldb, X, c->nx, ldX, N));
     T32* bufs[3] = {c->wbuf[0].as<T32>(), c->wbuf[1].as<T32>(), c->wbuf[2].as<T32>()};
-    const T32* ys = nullptr;
-    LYNX_TRY(filter_blocks<T32>(c, *nxp, X32, *ldb, bufs, *ldb, Vp, N, lc, emin, emax, degree, use_k, Y, &ys));
-    if (want_hy) {
-        *HY = (*Y == bufs[0]) ? bufs[1] : bufs[0];
-        LYNX_TRY(cheb_step<T32>(c, *nxp, *Y, *ldb, nullptr, 0, *HY, *ldb, Vp, N, 1.0, 0.0, 0.0, use_k, ys));
+    // Column blocks: every column is filtered independently, so blocks give bitwise the same
+    // result; a block waits for the event that marks its arrival (host-pointer solve), and the
+    // copies of later blocks overlap the filtering of earlier ones.
+    std::vector<std::pair<int, cudaEvent_t>> blocks = c->col_blocks;
+    if (blocks.empty()) blocks.push_back({0, nullptr});
+    for (size_t bi = 0; bi < blocks.size(); ++bi) {
+        const int b0 = blocks[bi].first;
+        const int nb = (bi + 1 < blocks.size() ? blocks[bi + 1].first : N) - b0;
+        if (blocks[bi].second) LYNX_CUDA_TRY(cudaStreamWaitEvent(c->stream, blocks[bi].second, 0));
+        const long long o = (long long)b0 * (*ldb);
+        LYNX_TRY(repack<T32, T64>(c, X32 + o, *nxp, *ldb, X + (long long)b0 * ldX, c->nx, ldX, nb));
+        T32* bb[3] = {bufs[0] + o, bufs[1] + o, bufs[2] + o};
+        T32* yb = nullptr;
+        const T32* ys = nullptr;
+        LYNX_TRY(filter_blocks<T32>(c, *nxp, X32 + o, *ldb, bb, *ldb, Vp, nb, lc, emin, emax, degree, use_k, &yb, &ys));
+        const int iy = (yb == bb[0]) ? 0 : (yb == bb[1] ? 1 : 2);  // the same buffer for every block
+        *Y = bufs[iy];
+        if (want_hy) {
+            *HY = (iy == 0) ? bufs[1] : bufs[0];
+            LYNX_TRY(cheb_step<T32>(c, *nxp, yb, *ldb, nullptr, 0, *HY + o, *ldb, Vp, nb, 1.0, 0.0, 0.0, use_k, ys));
+        }
     }
     return LYNX_OK;
 }
@@ -1321,6 +1340,7 @@ int lynx_destroy(lynx_ctx* c) {
     c->fbeta.release();
     c->fwork.release();
     c->fones.release();
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (auto& b : c->nl_layout_bufs) b.release();
     for (auto& kv : c->nl_maps) {
         kv.second.ptmap.release();
@@ -1691,10 +1711,40 @@ int lynx_eigensolver_solve_host(lynx_ctx* c, double* psi, double* eig, const dou
     DevBuf& dv = c->io_v;
     LYNX_TRY(dpsi.ensure(sizeof(double) * (size_t)Nd * nband));
     LYNX_TRY(dv.ensure(sizeof(double) * (size_t)Nd));
-    LYNX_CUDA_TRY(cudaMemcpy2DAsync(dpsi.p, Nd * 8, psi, l * 8, Nd * 8, nband, cudaMemcpyHostToDevice, c->stream));
     LYNX_CUDA_TRY(cudaMemcpyAsync(dv.p, veff, Nd * 8, cudaMemcpyHostToDevice, c->stream));
+    // Mixed precision, real, pipelined layout: copy psi in blocks of 128 columns on a second
+    // stream; the filter starts on a block as soon as it has landed (see run_filter32).
+    const bool pipelined = precision == LYNX_PREC_MIXED && pipe_capable<float>(c->nx) && nband >= 256;
+    std::vector<cudaEvent_t> evs;
+    if (pipelined) {
+        if (!c->copy_stream) LYNX_CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        cudaEvent_t start;
+        LYNX_CUDA_TRY(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+        evs.push_back(start);
+        LYNX_CUDA_TRY(cudaEventRecord(start, c->stream));  // earlier work on the stream is done with dpsi
+        LYNX_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, start, 0));
+        c->col_blocks.clear();
+        for (int b0 = 0; b0 < nband;) {
+            const int nb = (nband - b0 <= 192) ? nband - b0 : 128;
+            cudaEvent_t ev;
+            LYNX_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+            evs.push_back(ev);
+            LYNX_CUDA_TRY(cudaMemcpy2DAsync(dpsi.as<double>() + (size_t)b0 * Nd, Nd * 8, psi + (size_t)b0 * l, l * 8,
+                                            Nd * 8, nb, cudaMemcpyHostToDevice, c->copy_stream));
+            LYNX_CUDA_TRY(cudaEventRecord(ev, c->copy_stream));
+            c->col_blocks.push_back({b0, ev});
+            b0 += nb;
+        }
+    } else {
+        LYNX_CUDA_TRY(cudaMemcpy2DAsync(dpsi.p, Nd * 8, psi, l * 8, Nd * 8, nband, cudaMemcpyHostToDevice, c->stream));
+    }
     int st = lynx_eigensolver_solve(c, dpsi.as<double>(), eig, dv.as<double>(), nband, (int)Nd, lc, emin, emax,
                                     degree, precision, lc_out);
+    c->col_blocks.clear();
+    if (pipelined) {
+        cudaStreamSynchronize(c->copy_stream);
+        for (cudaEvent_t e : evs) cudaEventDestroy(e);
+    }
     if (st == LYNX_OK) {
         cudaError_t e = cudaMemcpy2DAsync(psi, l * 8, dpsi.p, Nd * 8, Nd * 8, nband, cudaMemcpyDeviceToHost, c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

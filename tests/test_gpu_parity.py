@@ -267,3 +267,24 @@ def test_fused_nonlocal_and_shapes_bitwise(system):
         ref_ = out[(0, 0, prec)]
         for key in ((0, 1), (1, 0), (1, 1)):
             assert np.array_equal(out[key + (prec,)], ref_), (key, prec)
+
+
+def test_host_solve_pipelined_matches_device(system):
+    """lynx_eigensolver_solve_host copies psi in column blocks on a second stream and filters
+    each block as it lands (mixed precision, >= 256 states): bitwise the device-pointer pass."""
+    import ctypes
+    from lynx_b200 import _lib
+    s = system
+    lo, hi, lc = _bounds(s)
+    N = 300
+    psi0 = C.random_orbitals(s["ctx"].nd, N, seed=201)
+    hp = np.asfortranarray(psi0.copy())
+    eig_h = np.zeros(N)
+    V = np.ascontiguousarray(s["V"], dtype=np.float64)
+    lco = ctypes.c_double()
+    _lib.check(s["ctx"].lib.lynx_eigensolver_solve_host(s["ctx"].handle, _lib.dptr(hp), _lib.dptr(eig_h), _lib.dptr(V),
+                                                       N, s["ctx"].nd, lc, lo, hi, 8, _lib.PREC_MIXED,
+                                                       ctypes.byref(lco)))
+    psi_d, eig_d = s["solver"].EigenSolver(s["ctx"], "mixed").solve(psi0, s["V"], lc, lo, hi, 8)
+    assert np.array_equal(eig_h, np.asarray(eig_d))
+    assert np.array_equal(hp, np.asarray(psi_d))
