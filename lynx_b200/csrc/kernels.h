@@ -62,8 +62,8 @@ template <typename T, typename S>
 int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, const T* xold, long long ldo, T* out,
                      long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl, const T* phr,
                      int* err, cudaStream_t st, int shape = 0, const struct PipeNLHost* nlh = nullptr);
-// Number of launch shapes compiled for FD half-width R (shape indices 0 .. count-1; any shape
-// gives bitwise the same result, they differ in speed only).
+// Number of launch shapes for FD half-width R: compiled shapes x two y-band splits (shape
+// indices 0 .. count-1; any shape gives bitwise the same result, they differ in speed only).
 template <typename T>
 int pipe_shape_count(int R);
 

@@ -173,6 +173,9 @@ struct lynx_ctx {
     bool autotune = true;     // time the compiled stencil launch shapes on first use per grid
     std::map<std::array<long long, 7>, int> pipe_shape;  // chosen launch shape per (type, grid, columns, fused)
     bool fuse_nl = false;     // add the nonlocal term inside the stencil when the spheres are disjoint
+    // with fuse_nl: the stencil also writes compact sphere-point copies of its output and the
+    // next step gathers from them (measured slower than the direct gather on B200: off)
+    bool fuse_compact_gather = false;
     struct NLMap {
         DevBuf ptmap, rowstart;
         std::vector<int> rowstart_h;
@@ -676,7 +679,9 @@ int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, lo
 template <typename T>
 int compact_bufs(lynx_ctx* c, int ncol, T* xs[2]) {
     xs[0] = xs[1] = nullptr;
-    if (ScalarOf<T>::cplx || !c->has_nl || !c->fuse_nl || !c->nl.compact || c->nl.n_colors != 1) return LYNX_OK;
+    if (ScalarOf<T>::cplx || !c->has_nl || !c->fuse_nl || !c->fuse_compact_gather || !c->nl.compact ||
+        c->nl.n_colors != 1)
+        return LYNX_OK;
     const long long ldw = ((long long)c->nl.n_pts + 3) & ~3LL;
     for (int i = 0; i < 2; ++i) {
         LYNX_TRY(c->xsbuf[i].ensure(sizeof(T) * (size_t)ldw * ncol));

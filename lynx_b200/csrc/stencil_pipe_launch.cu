@@ -111,7 +111,8 @@ bool phases_trivial(const T* phl, const T* phr) {
 
 template <typename T>
 int pipe_shape_count(int R) {
-    return (R == kTunedR) ? NumShapes<T>::value : 1;
+    // shapes x band splits: index = shape + NumShapes * (extra y-bands, 0 or 1)
+    return (R == kTunedR && NumShapes<T>::value > 1) ? 2 * NumShapes<T>::value : 1;
 }
 
 template <typename T, typename S>
@@ -126,7 +127,9 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
         set_error("fused nonlocal term needs real data, periodic cells and FD order 12");
         return LYNX_ERR_UNSUPPORTED;
     }
-    const int si = (shape > 0 && shape < pipe_shape_count<T>(R) && !phased) ? shape : 0;
+    const int sidx = (shape > 0 && shape < pipe_shape_count<T>(R) && !phased) ? shape : 0;
+    const int si = sidx % NumShapes<T>::value;    // compiled launch shape
+    const int extra_bands = sidx / NumShapes<T>::value;  // one more y-band: more, shorter CTAs
     const ShapeRT sh = shape_rt<T>(si);
     const int RX = sh.RX, RY = sh.RY, MT = sh.MAXT;
     if (R < 1 || R > 8) {
@@ -158,9 +161,9 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
     TYT = std::min(TYT, (MT - 32) / P2);
     TYT = std::min(TYT, (g.ny + RY - 1) / RY);
     {
-        const int nb = (g.ny + TYT * RY - 1) / (TYT * RY);
+        const int nb = std::min(g.ny, (g.ny + TYT * RY - 1) / (TYT * RY) + extra_bands);
         const int ty_bal = (g.ny + nb - 1) / nb;
-        TYT = std::min(TYT, (ty_bal + RY - 1) / RY);
+        TYT = std::max(1, std::min(TYT, (ty_bal + RY - 1) / RY));
     }
     const int nthr = ((P2 * TYT + 31) / 32) * 32 + 32;  // consumer warps + one producer warp
     PipeGeom G;
