@@ -156,6 +156,20 @@ LYNX_API int lynx_eigensolver_solve_host(lynx_ctx* ctx, double* psi, double* eig
                                 int ld, double lambda_cutoff, double eigmin, double eigmax, int degree,
                                 int precision, double* lambda_cutoff_out);
 
+/* Batched CheFSI passes: nb independent problems (the k-points and spins of one cell, or the
+ * cells of an ensemble, on grids of any sizes), problem i on context ctxs[i] with device
+ * orbitals psi[i] (complex interleaved when is_kpt[i], at that context's k-point), host
+ * eigenvalues eig[i] and device potential veff[i]; the other arrays give each problem's nband,
+ * ld, lambda_cutoff, eigmin, eigmax, and lambda_cutoff_out (may be NULL).  The passes run
+ * concurrently, one host thread per problem, so give every context its own stream
+ * (lynx_set_stream); problems sharing a context or a stream are serialised.  Returns the first
+ * failing status (in problem order).  Replaces the reference's loop over (spin, k-point) in
+ * SCF::solve_eigenproblem (src/scf/SCF.cpp:383-410) around EigenSolver::solve / solve_kpt. */
+LYNX_API int lynx_eigensolver_solve_batch(lynx_ctx** ctxs, int nb, double** psi, double** eig, const double** veff,
+                                          const int* nband, const int* ld, const double* lambda_cutoff,
+                                          const double* eigmin, const double* eigmax, const int* is_kpt, int degree,
+                                          int precision, double* lambda_cutoff_out);
+
 /* Extreme eigenvalue estimates of H by Lanczos (tolerance on both ends, at most max_iter steps,
  * fixed seed), returned with the reference's safety margins (max*1.01, min-0.1).  Device veff.
  * Replaces EigenSolver::lanczos_bounds / lanczos_bounds_kpt (src/solvers/EigenSolver.hpp:43-45,55-58;

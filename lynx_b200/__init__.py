@@ -12,12 +12,14 @@ __all__ = [
     "cell", "pseudo", "Cell", "diamond_si", "fcc_si_primitive", "kpoints_mp", "random_orbitals",
     "synthetic_veff", "NonlocalTables", "nonlocal_tables", "read_psp8", "synthetic_si_psp8",
     "Context", "Hamiltonian", "EigenSolver", "NonlocalProjector", "fermi_level", "occupations",
+    "solve_batch",
 ]
 
 
 def __getattr__(name):
     # The operator classes load liblynxb200.so on first use.
-    if name in ("Context", "Hamiltonian", "EigenSolver", "NonlocalProjector", "fermi_level", "occupations"):
+    if name in ("Context", "Hamiltonian", "EigenSolver", "NonlocalProjector", "fermi_level", "occupations",
+                "solve_batch"):
         from . import solver
         return getattr(solver, name)
     raise AttributeError(name)

@@ -64,6 +64,7 @@ _SIGNATURES = {
     "lynx_nonlocal_apply": (_c_int, [_p, _p, _p, _c_int, _c_int]),
     "lynx_nonlocal_apply_noalloc": (_c_int, [_p, _p, _p, _c_int, _c_int]),
     "lynx_set_option": (_c_int, [_p, _c_int, _c_int]),
+    "lynx_eigensolver_solve_batch": (_c_int, [_p, _c_int, _p, _p, _p, _p, _p, _p, _p, _p, _p, _c_int, _c_int, _p]),
     "lynx_nonlocal_force": (_c_int, [_p, _p, _c_int, _c_int, _p, ctypes.c_double, _p, _p]),
     "lynx_nonlocal_force_kpt": (_c_int, [_p, _p, _c_int, _c_int, _p, ctypes.c_double, _p, _p]),
     "lynx_nonlocal_apply_kpt": (_c_int, [_p, _p, _p, _c_int, _c_int]),

@@ -352,15 +352,16 @@ __global__ void gram_reduce_kernel(double* __restrict__ Ms, double* __restrict__
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
+    // looked up once; thread-safe (function-local static initialisation)
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
         cudaDriverEntryPointQueryResult q;
         void* p = nullptr;
         if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
                 cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        return nullptr;
+    }();
     return fn;
 }
 
@@ -725,7 +726,7 @@ int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows
     g.ws = ws;
     g.err = err;
     const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
-    LYNX_CUDA_TRY(cudaFuncSetAttribute(gram_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LYNX_CUDA_TRY(smem_cap(gram_i8_kernel, smem));
     dim3 grid(g.ntri + g.T * g.T, p.nsplit);
     gram_i8_kernel<<<grid, 128, smem, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], g);
     {
@@ -778,8 +779,7 @@ int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp
     int* erow = reinterpret_cast<int*>(w + 3 * p.a_bytes + 3 * p.b_bytes);
     int* dcol = reinterpret_cast<int*>(w + 3 * p.a_bytes + 3 * p.b_bytes + p.erow_bytes);
     double* fpow = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(dcol) + p.col_bytes);
-    LYNX_CUDA_TRY(cudaFuncSetAttribute(slice_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)p.smem_rows));
+    LYNX_CUDA_TRY(smem_cap(slice_rows_kernel, p.smem_rows));
     slice_rows_kernel<<<(unsigned)((rows + 31) / 32), 256, p.smem_rows, st>>>(a[0], a[1], a[2], p.ldk, erow, Y, ldy,
                                                                                rows, n, dcol);
     slice_w_kernel<<<n, 128, 0, st>>>(b[0], b[1], b[2], p.ldk, fpow, W, n, dcol);
@@ -800,7 +800,7 @@ int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp
     g.ldp = ldp;
     g.err = err;
     const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
-    LYNX_CUDA_TRY(cudaFuncSetAttribute(rot_i8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LYNX_CUDA_TRY(smem_cap(rot_i8_kernel, smem));
     const long long ntm = (rows + BM - 1) / BM;
     rot_i8_kernel<<<(unsigned)(ntm * g.ntn), 128, smem, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], g);
     count_launch();

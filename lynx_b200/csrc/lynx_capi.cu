@@ -22,8 +22,10 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <mutex>
 #include <type_traits>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.h"
@@ -45,6 +47,21 @@ void set_error(const char* fmt, ...) {
 }
 
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+cudaError_t raise_smem_cap(const void* func, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;  // below the default cap
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> caps;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cap = caps[{dev, func}];
+    if (bytes <= cap) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) cap = bytes;
+    return e;
+}
 
 // Growable device buffer.
 struct DevBuf {
@@ -1957,6 +1974,44 @@ extern "C" int lynx_nonlocal_force_kpt(lynx_ctx* c, const double* psi_z, int nba
                                        double spn_fac_wk, double* force, double* energy_nl) {
     return nonlocal_force_impl<double2>(c, reinterpret_cast<const double2*>(psi_z), nband, ld, occ, spn_fac_wk,
                                         0.5 * spn_fac_wk, force, energy_nl, true);
+}
+
+extern "C" int lynx_eigensolver_solve_batch(lynx_ctx** ctxs, int nb, double** psi, double** eig,
+                                            const double** veff, const int* nband, const int* ld,
+                                            const double* lambda_cutoff, const double* eigmin, const double* eigmax,
+                                            const int* is_kpt, int degree, int precision,
+                                            double* lambda_cutoff_out) {
+    LYNX_CHECK_ARG(nb >= 0, "negative batch size");
+    if (nb == 0) return LYNX_OK;
+    LYNX_CHECK_ARG(ctxs && psi && eig && veff && nband && ld && lambda_cutoff && eigmin && eigmax && is_kpt,
+                   "null pointer");
+    for (int i = 0; i < nb; ++i) LYNX_CHECK_ARG(ctxs[i] != nullptr, "null context in the batch");
+    std::vector<int> st(nb, LYNX_OK);
+    std::vector<std::string> msg(nb);
+    // problems that share a context run one after another on the same thread
+    std::map<lynx_ctx*, std::vector<int>> groups;
+    for (int i = 0; i < nb; ++i) groups[ctxs[i]].push_back(i);
+    auto run = [&](const std::vector<int>& idx) {
+        for (int i : idx) {
+            double* lco = lambda_cutoff_out ? lambda_cutoff_out + i : nullptr;
+            st[i] = is_kpt[i] ? lynx_eigensolver_solve_kpt(ctxs[i], psi[i], eig[i], veff[i], nband[i], ld[i],
+                                                           lambda_cutoff[i], eigmin[i], eigmax[i], degree, precision,
+                                                           lco)
+                              : lynx_eigensolver_solve(ctxs[i], psi[i], eig[i], veff[i], nband[i], ld[i],
+                                                       lambda_cutoff[i], eigmin[i], eigmax[i], degree, precision, lco);
+            if (st[i] != LYNX_OK) msg[i] = lynx_last_error();
+        }
+    };
+    std::vector<std::thread> th;
+    th.reserve(groups.size());
+    for (auto& g : groups) th.emplace_back(run, std::cref(g.second));
+    for (auto& t : th) t.join();
+    for (int i = 0; i < nb; ++i)
+        if (st[i] != LYNX_OK) {
+            set_error("batch problem %d: %s", i, msg[i].c_str());
+            return st[i];
+        }
+    return LYNX_OK;
 }
 
 extern "C" int lynx_set_option(lynx_ctx* c, int option, int value) {

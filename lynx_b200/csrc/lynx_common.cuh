@@ -15,6 +15,17 @@ constexpr int kMaxRadius = 8;
 // Per-thread error string, returned by lynx_last_error().
 void set_error(const char* fmt, ...);
 
+// Raises a kernel's dynamic shared-memory cap (cudaFuncAttributeMaxDynamicSharedMemorySize) to at
+// least `bytes`.  The cap is one value per function and device for the whole process, and host
+// threads solving different grids launch the same kernel with different sizes at once: a thread
+// that lowered it would make another thread's larger launch fail.  So the cap only grows, under
+// a lock.
+cudaError_t raise_smem_cap(const void* func, size_t bytes);
+template <typename K>
+cudaError_t smem_cap(K* kern, size_t bytes) {
+    return raise_smem_cap(reinterpret_cast<const void*>(kern), bytes);
+}
+
 }  // namespace lynxb
 
 #define LYNX_CUDA_TRY(...)                                                                      \

@@ -47,7 +47,7 @@ template <typename T, int NPG>
 int gather2(const NLDev& nl, const T* x, long long ld, int ncol, T* alpha, int ncolp, double dV, cudaStream_t st) {
     const size_t smem = Gather2Geom<T, NPG>::smem_bytes;
     auto kern = nl_gather2_kernel<T, NPG>;
-    if (smem > 48 * 1024) LYNX_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LYNX_CUDA_TRY(smem_cap(kern, smem));
     dim3 grid(nl.n_atom, (ncol + kNL2Cols - 1) / kNL2Cols);
     kern<<<grid, 256, smem, st>>>(x, ld, ncol, ncolp, make_view<T>(nl), alpha, dV);
     count_launch();
@@ -88,7 +88,7 @@ int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alp
     const size_t smem = sizeof(T) * kGatherTile * (NB + 1) + sizeof(S) * nl.max_np * kGatherTile;
     dim3 grid(nl.n_atom, (ncol + NB - 1) / NB);
     auto go = [&](auto kern) {
-        if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        smem_cap(kern, smem);
         kern<<<grid, 256, smem, st>>>(x, ld, ncol, ncolp, make_view<T>(nl), alpha, dV);
     };
     if (pj <= 1) go(nl_gather_kernel<T, NB, 1>);

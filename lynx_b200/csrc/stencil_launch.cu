@@ -20,7 +20,7 @@ void launch_one(dim3 grid, int nthr, size_t smem, cudaStream_t st, const T* x, c
                 const typename ScalarOf<T>::type* V, const StencilArgs<T>& A) {
     constexpr int RY = rows_per_thread<T>();
     auto kern = cheb_step_kernel<T, R, RY, HK, XOLD>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_cap(kern, smem);
     kern<<<grid, nthr, smem, st>>>(x, xold, out, V, A);
 }
 

@@ -62,7 +62,7 @@ void launch_pipe_ph(int ns, dim3 grid, int nthr, size_t smem, cudaStream_t st, c
     auto kern = ns >= 5 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 5, PH, MT, NLF>
                : (ns == 4 ? cheb_pipe_kernel<T, R, RX, RY, XOLD, 4, PH, MT, NLF>
                           : cheb_pipe_kernel<T, R, RX, RY, XOLD, 3, PH, MT, NLF>);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_cap(kern, smem);
     kern<<<grid, nthr, smem, st>>>(x, xo, out, V, G, C, NL, err);
 }
 

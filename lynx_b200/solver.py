@@ -97,6 +97,14 @@ class Context:
         s = torch.cuda.current_stream(self.device).cuda_stream
         check(self.lib.lynx_set_stream(self._h, ctypes.c_void_p(s)))
 
+    def set_stream(self, stream):
+        """Put the context's work on `stream` (a torch.cuda.Stream or a raw cudaStream_t)."""
+        raw = getattr(stream, "cuda_stream", stream)
+        check(self.lib.lynx_set_stream(self._h, ctypes.c_void_p(int(raw))))
+
+    def set_option(self, option: int, value: int):
+        check(self.lib.lynx_set_option(self._h, int(option), int(value)))
+
     def stencil_coeffs(self) -> dict:
         n = self.cell.fd_order // 2 + 1
         out = {k: np.zeros(n) for k in ("D2x", "D2y", "D2z", "D2xy", "D2xz", "D2yz", "D1x", "D1y", "D1z")}
@@ -337,3 +345,63 @@ def occupations(eigs, ef: float, beta: float, smearing: str = "fermi-dirac") -> 
     occ = np.zeros_like(e)
     check(lib.lynx_occupations(dptr(e), len(e), float(ef), float(beta), _SMEAR[smearing], dptr(occ)))
     return occ
+
+
+def solve_batch(solvers, psis, Veffs, lambda_cutoffs, eigval_mins, eigval_maxs, cheb_degree: int = 20,
+                precision: Optional[str] = None, kpt=False):
+    """One CheFSI pass of several independent problems at once (lynx_eigensolver_solve_batch).
+
+    Problem i is solvers[i].solve (or solve_kpt when kpt[i]) on psis[i] with Veffs[i]; the
+    problems are the k-points and spins of one cell or the cells of an ensemble, each on its
+    own Context.  Every distinct context gets a stream of its own for the call, and the passes
+    run concurrently from host threads.  Returns [(psi_out, eig)], in order, as solve does;
+    each solver's lambda_cutoff is updated."""
+    torch = _torch()
+    nb = len(solvers)
+    kflags = [bool(k) for k in (kpt if isinstance(kpt, (list, tuple)) else [kpt] * nb)]
+    if not (len(psis) == len(Veffs) == len(lambda_cutoffs) == len(eigval_mins) == len(eigval_maxs) ==
+            len(kflags) == nb):
+        raise ValueError("solve_batch: every per-problem list must have one entry per solver")
+    if nb == 0:
+        return []
+    prec = _PREC[precision or solvers[0].precision]
+    args = [_DeviceArgs(sv.ctx, p, k) for sv, p, k in zip(solvers, psis, kflags)]
+    vs = [_veff_dev(sv.ctx, V) for sv, V in zip(solvers, Veffs)]
+    eigs = [np.zeros(a.ncol) for a in args]
+    # inputs were written on the current streams; the passes run on streams of their own
+    for dev in {sv.ctx.device for sv in solvers}:
+        torch.cuda.current_stream(dev).synchronize()
+    streams = {}
+    for sv in solvers:
+        h = sv.ctx.handle.value
+        if h not in streams:
+            streams[h] = torch.cuda.Stream(device=sv.ctx.device)
+            sv.ctx.set_stream(streams[h])
+    P = ctypes.c_void_p * nb
+    I = ctypes.c_int * nb
+    D = ctypes.c_double * nb
+    ctxs = P(*[sv.ctx.handle.value for sv in solvers])
+    psi_p = P(*[_dev_ptr(a.t) for a in args])
+    eig_p = P(*[e.ctypes.data for e in eigs])
+    v_p = P(*[v.data_ptr() for v in vs])
+    nband = I(*[a.ncol for a in args])
+    ld = I(*[sv.ctx.nd for sv in solvers])
+    lc = D(*[float(x) for x in lambda_cutoffs])
+    lo = D(*[float(x) for x in eigval_mins])
+    hi = D(*[float(x) for x in eigval_maxs])
+    isk = I(*[1 if k else 0 for k in kflags])
+    lc_out = D()
+    lib = solvers[0].ctx.lib
+    try:
+        check(lib.lynx_eigensolver_solve_batch(ctxs, nb, psi_p, eig_p, v_p, nband, ld, lc, lo, hi, isk,
+                                               int(cheb_degree), prec, lc_out))
+    finally:
+        for st in streams.values():
+            st.synchronize()
+        for sv in solvers:
+            sv.ctx.sync_stream()
+    out = []
+    for i, (sv, a) in enumerate(zip(solvers, args)):
+        sv._lambda_cutoff = lc_out[i]
+        out.append((a.out(a.t), eigs[i]))
+    return out
