@@ -123,6 +123,12 @@ struct NLDev {
     int2* pt_meta = nullptr;     // [n_pts] (first projector row, projector count) of the point's atom
     double* chi_pt64 = nullptr;  // [max_np][n_pts] projector values in point order
     float* chi_pt32 = nullptr;
+    // Tiles of kExpTilePts consecutive points for the expansion kernel: the distinct atoms of
+    // tile t in order of first appearance, exp_tile_atoms[t * exp_amax + slot] (-1 past the
+    // tile's count), and every point's slot in its tile.
+    int exp_amax = 0;
+    int* exp_tile_atoms = nullptr;
+    unsigned char* pt_slot = nullptr;
     int* atom_img_ptr = nullptr;
     int* atom_img_list = nullptr;
     int* atom_nproj = nullptr;
@@ -144,6 +150,8 @@ struct NLDev {
 
 // Column block widths of the nonlocal kernels; alpha rows are padded to a multiple of kNLColBlock.
 constexpr int kNLColBlock = 32;
+// Points per tile (= threads per CTA) of the compact expansion kernel.
+constexpr int kExpTilePts = 256;
 
 template <typename T>
 int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alpha, int ncolp, double dV,

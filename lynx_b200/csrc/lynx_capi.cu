@@ -1573,6 +1573,33 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
             }
             LYNX_TRY(up(ent_pt.data(), ent_pt.size() * 4, (void**)&d.ent_pt));
             LYNX_TRY(up(pt_meta.data(), pt_meta.size() * 4, (void**)&d.pt_meta));
+            {
+                // expansion tiles: distinct atoms of every kExpTilePts consecutive points
+                const long long ntile = (tot + kExpTilePts - 1) / kExpTilePts;
+                std::vector<std::vector<int>> tatoms(ntile);
+                std::vector<unsigned char> slot(tot);
+                int amax = 0;
+                for (long long t = 0; t < ntile; ++t) {
+                    auto& at = tatoms[t];
+                    for (long long s2 = t * kExpTilePts; s2 < std::min<long long>(tot, (t + 1) * kExpTilePts); ++s2) {
+                        const long long k = keys[s2] & 0xFFFFFFFFLL;
+                        const int a = img_atom[owner_img[k]];
+                        auto f = std::find(at.begin(), at.end(), a);
+                        if (f == at.end()) {
+                            at.push_back(a);
+                            f = at.end() - 1;
+                        }
+                        slot[s2] = (unsigned char)(f - at.begin());
+                    }
+                    amax = std::max(amax, (int)at.size());
+                }
+                std::vector<int> flat((size_t)ntile * amax, -1);
+                for (long long t = 0; t < ntile; ++t)
+                    std::copy(tatoms[t].begin(), tatoms[t].end(), flat.begin() + t * amax);
+                d.exp_amax = amax;
+                LYNX_TRY(up(flat.data(), flat.size() * 4, (void**)&d.exp_tile_atoms));
+                LYNX_TRY(up(slot.data(), slot.size(), (void**)&d.pt_slot));
+            }
             LYNX_TRY(up(cp64.data(), cp64.size() * 8, (void**)&d.chi_pt64));
             LYNX_TRY(up(cp32.data(), cp32.size() * 4, (void**)&d.chi_pt32));
         }

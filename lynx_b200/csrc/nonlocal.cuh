@@ -563,6 +563,61 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// The same expansion with the alpha rows of a tile's atoms staged in shared memory.  CTA = one
+// tile of kExpTilePts consecutive points x one 128-byte column block (CB columns); thread = one
+// point.  Consecutive points in grid order cross several spheres, so the lanes of a warp need
+// different atoms' rows: read from global memory those requests serialise in L1 (the kernel
+// above is L1-bound), from shared memory they do not.  Row r (slot * max_np + j) holds 8 chunks
+// of 16 bytes, chunk q stored at position q ^ (r & 7), so lanes reading different atoms' rows in
+// one instruction hit different banks.  Sums in the order of the kernel above.
+template <typename T>
+__global__ void __launch_bounds__(kExpTilePts)
+    nl_expand_tile_kernel(T* __restrict__ W, long long ldw, int ncol, int ncolp, int n_pts,
+                          const T* __restrict__ chi_pt, const int2* __restrict__ pt_meta,
+                          const unsigned char* __restrict__ pt_slot, const int* __restrict__ tile_atoms, int amax,
+                          int max_np, const int* __restrict__ atom_poff, const int* __restrict__ atom_nproj,
+                          const T* __restrict__ alpha) {
+    constexpr int VW = 16 / (int)sizeof(T);  // elements per chunk
+    constexpr int CB = 8 * VW;               // columns per CTA
+    extern __shared__ __align__(16) unsigned char smx[];
+    float4* rows = reinterpret_cast<float4*>(smx);
+    const int t = blockIdx.x, n0 = blockIdx.y * CB;
+    const int* ta = tile_atoms + (long long)t * amax;
+    for (int e = threadIdx.x; e < amax * max_np * 8; e += blockDim.x) {
+        const int q = e & 7, r = e >> 3;
+        const int slot = r / max_np, j = r - slot * max_np;
+        const int a = ta[slot];
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (a >= 0 && j < atom_nproj[a])
+            v = *reinterpret_cast<const float4*>(alpha + (long long)(atom_poff[a] + j) * ncolp + n0 + q * VW);
+        rows[r * 8 + (q ^ (r & 7))] = v;
+    }
+    __syncthreads();
+    const int pt = t * kExpTilePts + threadIdx.x;
+    if (pt >= n_pts) return;
+    const int np = pt_meta[pt].y;
+    const int r0 = (int)pt_slot[pt] * max_np;
+    T acc[CB];
+#pragma unroll
+    for (int k = 0; k < CB; ++k) acc[k] = T(0);
+#pragma unroll 2
+    for (int j = 0; j < np; ++j) {
+        const T c = chi_pt[(long long)j * n_pts + pt];
+        const int r = r0 + j;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float4 raw = rows[r * 8 + (q ^ (r & 7))];
+            const T* v = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+            for (int k = 0; k < VW; ++k) acc[q * VW + k] = fma(c, v[k], acc[q * VW + k]);
+        }
+    }
+    T* wp = W + (long long)n0 * ldw + pt;
+#pragma unroll
+    for (int k = 0; k < CB; ++k)
+        if (n0 + k < ncol) wp[(long long)k * ldw] = acc[k];
+}
+
 // Nonlocal force reduction for one direction (src/physics/Forces.cpp:772-777, :682-684):
 //   force[a * 3 + dim] = -spn * sum_n occ[n] sum_{j < np(a)} Gamma[poff+j] Re(conj(alpha) beta)
 // and, for dim == 0, the atom's energy share  ea[a] = efac * sum_n occ[n] sum_j Gamma |alpha|^2.
