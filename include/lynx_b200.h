@@ -226,9 +226,10 @@ LYNX_API int lynx_nonlocal_apply_noalloc(lynx_ctx* ctx, const double* psi, doubl
  *   LYNX_OPT_AUTOTUNE:       1 (default) times the compiled stencil launch shapes on the first
  *                            launch for each grid and column count and keeps the fastest; 0 uses
  *                            the default shape.
- *   LYNX_OPT_FUSE_NONLOCAL:  1 adds the nonlocal term inside the stencil kernel when the
- *                            projector spheres are disjoint (compact per-point copies between
- *                            steps); 0 (default) uses the separate gather and scatter kernels. */
+ *   LYNX_OPT_FUSE_NONLOCAL:  1 (default) adds the nonlocal term inside the stencil kernel when
+ *                            the projector spheres are disjoint (real data, periodic orthogonal
+ *                            cell, FD order 12), from a compact per-point expansion; 0 always
+ *                            uses the separate gather and scatter kernels. */
 enum { LYNX_OPT_AUTOTUNE = 1, LYNX_OPT_FUSE_NONLOCAL = 2 };
 LYNX_API int lynx_set_option(lynx_ctx* ctx, int option, int value);
 

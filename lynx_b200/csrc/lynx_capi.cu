@@ -189,7 +189,7 @@ struct lynx_ctx {
     bool no_tc_gram = false;  // diagnostic switch: FP64 library products for the mixed path
     bool autotune = true;     // time the compiled stencil launch shapes on first use per grid
     std::map<std::array<long long, 7>, int> pipe_shape;  // chosen launch shape per (type, grid, columns, fused)
-    bool fuse_nl = false;     // add the nonlocal term inside the stencil when the spheres are disjoint
+    bool fuse_nl = true;      // add the nonlocal term inside the stencil when the spheres are disjoint
     // with fuse_nl: the stencil also writes compact sphere-point copies of its output and the
     // next step gathers from them (measured slower than the direct gather on B200: off)
     bool fuse_compact_gather = false;
