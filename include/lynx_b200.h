@@ -195,6 +195,26 @@ LYNX_API int lynx_nonlocal_force(lynx_ctx* ctx, const double* psi, int nband, in
 LYNX_API int lynx_nonlocal_force_kpt(lynx_ctx* ctx, const double* psi_z, int nband, int ld, const double* occ,
                                      double spn_fac_wk, double* force, double* energy_nl);
 
+/* Kinetic and nonlocal stress of device psi (nband columns, leading dimension ld), before the
+ * division by the cell measure, Voigt order xx, xy, xz, yy, yz, zz:
+ *   stress_k[ab]  = -occfac dV sum_n occ[n] <D_a psi_n, D_b psi_n>,
+ *   stress_nl[ab] = -2 occfac sum_n occ[n] sum_p Gamma_p alpha_{p,n} beta^{ab}_{p,n} - delta_ab E_nl,
+ * D_a the Cartesian FD first derivative, alpha = dV chi^T psi, beta^{ab} = dV sum_g chi(g)
+ * (r_g - R_img)_b D_a psi(g) with the Cartesian position relative to the image centre, and
+ * E_nl = occfac sum_n occ[n] sum_p Gamma_p alpha^2.  img_pos: host, 3 doubles per image (the
+ * image centres of lynx_set_nonlocal, in the grid's coordinates: non-Cartesian for
+ * non-orthogonal cells); may be NULL without projectors.  stress_k, stress_nl: host, 6 doubles
+ * each.  Replaces Hamiltonian::compute_kinetic_nonlocal_stress_gpu
+ * (src/operators/Hamiltonian.hpp:156-160; the formula of src/physics/Stress.cpp:1041-1784). */
+LYNX_API int lynx_kinetic_nonlocal_stress(lynx_ctx* ctx, const double* psi, int nband, int ld, const double* occ,
+                                          double occfac, const double* img_pos, double* stress_k, double* stress_nl);
+/* Complex k-point version at the context's k-point (Bloch factors as in the nonlocal apply),
+ * with occfac replaced by spn_fac_wk / 2.  Replaces
+ * Hamiltonian::compute_kinetic_nonlocal_stress_kpt_gpu (src/physics/Stress.cpp:967-976). */
+LYNX_API int lynx_kinetic_nonlocal_stress_kpt(lynx_ctx* ctx, const double* psi_z, int nband, int ld,
+                                              const double* occ, double spn_fac_wk, const double* img_pos,
+                                              double* stress_k, double* stress_nl);
+
 /* Fermi level by Brent's method on sum_i w_i f(eps_i - Ef) = nelectron (tolerance 1e-14, <= 200
  * iterations), f Fermi-Dirac or Gaussian smearing.  Host arrays, FP64.
  * Replaces Occupation::find_fermi_level (src/electronic/Occupation.cpp:48-84). */

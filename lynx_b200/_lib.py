@@ -67,6 +67,8 @@ _SIGNATURES = {
     "lynx_eigensolver_solve_batch": (_c_int, [_p, _c_int, _p, _p, _p, _p, _p, _p, _p, _p, _p, _c_int, _c_int, _p]),
     "lynx_nonlocal_force": (_c_int, [_p, _p, _c_int, _c_int, _p, ctypes.c_double, _p, _p]),
     "lynx_nonlocal_force_kpt": (_c_int, [_p, _p, _c_int, _c_int, _p, ctypes.c_double, _p, _p]),
+    "lynx_kinetic_nonlocal_stress": (_c_int, [_p, _p, _c_int, _c_int, _p, ctypes.c_double, _p, _p, _p]),
+    "lynx_kinetic_nonlocal_stress_kpt": (_c_int, [_p, _p, _c_int, _c_int, _p, ctypes.c_double, _p, _p, _p]),
     "lynx_nonlocal_apply_kpt": (_c_int, [_p, _p, _p, _c_int, _c_int]),
     "lynx_chebyshev_filter": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _c_int]),
     "lynx_chebyshev_filter_kpt": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _c_int]),

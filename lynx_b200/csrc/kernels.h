@@ -168,6 +168,13 @@ int launch_nl_force_reduce(const NLDev& nl, const T* alpha, const T* beta, int n
 template <typename T>
 int launch_grad_dir(int nx, int ny, int nz, int nxp, int R, const double* D1, int dir, const T* x, long long ldx,
                     T* g, long long ldg, int ncol, const T* phl, const T* phr, cudaStream_t st);
+// Stress helpers (nonorth.cu): in-place Cartesian mixing of three lattice-direction gradient
+// blocks of n elements (uinv: 3x3 row-major uvec^-1), and the six Voigt products per column.
+template <typename T>
+int launch_cart_mix(T* g0, T* g1, T* g2, long long n, const double* uinv, cudaStream_t st);
+template <typename T>
+int launch_dot6(const T* g0, const T* g1, const T* g2, long long nd, long long ld, int ncol, double* out,
+                cudaStream_t st);
 // W[col * ldw + point] = (chi alpha)(point, col) on the compact point numbering (nl.compact).
 template <typename T>
 int launch_nl_expand(const NLDev& nl, T* W, long long ldw, int ncol, const T* alpha, int ncolp, cudaStream_t st);

@@ -211,6 +211,11 @@ struct lynx_ctx {
     std::map<int, NLDev> nl_layouts;
     std::vector<DevBuf> nl_layout_bufs;
     std::vector<int> h_gpos, h_pt_grid;  // host copies of the unpadded grid indices
+    // host copies for the stress: per-image offsets into gpos / chi, point counts, atoms; chi
+    std::vector<long long> h_img_goff, h_img_choff;
+    std::vector<int> h_img_ndc, h_img_atom, h_atom_nproj;
+    std::vector<double> h_chi;
+    DevBuf sbuf[4];  // stress: third gradient block, chi weighted by x, y, z relative positions
 };
 
 namespace {
@@ -1362,6 +1367,7 @@ int lynx_destroy(lynx_ctx* c) {
     c->fbeta.release();
     c->fwork.release();
     c->fones.release();
+    for (auto& b : c->sbuf) b.release();
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (auto& b : c->nl_layout_bufs) b.release();
     for (auto& kv : c->nl_maps) {
@@ -1626,6 +1632,12 @@ int lynx_set_nonlocal(lynx_ctx* c, int n_img, const int* img_atom, const int* im
     c->img_shift.assign(img_shift, img_shift + 3 * n_img);
     c->h_gpos.assign(gpos, gpos + tot);
     c->h_pt_grid = pt_grid;
+    c->h_img_goff = goff;
+    c->h_img_choff = choff;
+    c->h_img_ndc.assign(img_ndc, img_ndc + n_img);
+    c->h_img_atom.assign(img_atom, img_atom + n_img);
+    c->h_atom_nproj = nproj;
+    c->h_chi.assign(chi, chi + totchi);
     c->has_nl = true;
     return update_nl_phases(c);
 }
@@ -2001,6 +2013,144 @@ extern "C" int lynx_nonlocal_force_kpt(lynx_ctx* c, const double* psi_z, int nba
                                        double spn_fac_wk, double* force, double* energy_nl) {
     return nonlocal_force_impl<double2>(c, reinterpret_cast<const double2*>(psi_z), nband, ld, occ, spn_fac_wk,
                                         0.5 * spn_fac_wk, force, energy_nl, true);
+}
+
+// Kinetic and nonlocal stress of one (spin, k-point) block, un-normalised (Voigt xx, xy, xz, yy,
+// yz, zz), with of = occfac (Gamma) or spn_fac_wk / 2 (k-point):
+//   stress_k[ab]  = -of dV sum_n g_n Re <D_a psi_n, D_b psi_n>       (Cartesian FD gradients)
+//   stress_nl[ab] = -2 of sum_n g_n sum_j Gamma_j Re(conj(alpha_nj) beta^ab_nj) - delta_ab E_nl
+//   beta^ab = dV sum_img e^{-ik.R} chi (r - R_img)_b D_a psi,  E_nl = of sum g Gamma |alpha|^2
+// (src/physics/Stress.cpp:1041-1784; the GPU path's assembly src/physics/GPUForce.cu:471-680).
+// The relative positions enter through three copies of chi weighted by (r - R)_x, _y, _z, so
+// every beta is one gather of a gradient block; the sums over bands and atoms are finished on
+// the host in a fixed order.
+template <typename T>
+int stress_impl(lynx_ctx* c, const T* psi, int nband, int ld, const double* occ, double of, const double* img_pos,
+                double* stress_k, double* stress_nl, bool use_k) {
+    LYNX_CHECK_ARG(c && psi && occ && stress_k && stress_nl, "null pointer");
+    LYNX_CHECK_ARG(nband > 0, "nband must be positive");
+    const long long l = ld > 0 ? ld : c->Nd;
+    LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
+    LYNX_CHECK_ARG(!c->has_nl || img_pos, "image positions are required when projectors are set");
+    LYNX_TRY(activate(c));
+    const long long Nd = c->Nd;
+    const size_t gb = sizeof(T) * (size_t)Nd * nband;
+    LYNX_TRY(c->gradbuf[0].ensure(gb));
+    LYNX_TRY(c->gradbuf[1].ensure(gb));
+    LYNX_TRY(c->sbuf[0].ensure(gb));
+    T* G[3] = {c->gradbuf[0].as<T>(), c->gradbuf[1].as<T>(), c->sbuf[0].as<T>()};
+    T phl[3], phr[3];
+    ghost_phases<T>(c, use_k, phl, phr);
+    const double* D1[3] = {c->D1x.data(), c->D1y.data(), c->D1z.data()};
+    for (int d = 0; d < 3; ++d)
+        LYNX_TRY(launch_grad_dir<T>(c->nx, c->ny, c->nz, c->nx, geom(c).R, D1[d], d, psi, l, G[d], Nd, nband, phl, phr,
+                                    c->stream));
+    if (!c->orth) {
+        // Cartesian gradients: D_cart = uvec^-1 D_lattice
+        const double* u = c->uvec;
+        const double det = u[0] * (u[4] * u[8] - u[5] * u[7]) - u[1] * (u[3] * u[8] - u[5] * u[6]) +
+                           u[2] * (u[3] * u[7] - u[4] * u[6]);
+        LYNX_CHECK_ARG(std::fabs(det) > 1e-14, "singular lattice");
+        const double ui[9] = {(u[4] * u[8] - u[5] * u[7]) / det, (u[2] * u[7] - u[1] * u[8]) / det,
+                              (u[1] * u[5] - u[2] * u[4]) / det, (u[5] * u[6] - u[3] * u[8]) / det,
+                              (u[0] * u[8] - u[2] * u[6]) / det, (u[2] * u[3] - u[0] * u[5]) / det,
+                              (u[3] * u[7] - u[4] * u[6]) / det, (u[1] * u[6] - u[0] * u[7]) / det,
+                              (u[0] * u[4] - u[1] * u[3]) / det};
+        LYNX_TRY(launch_cart_mix<T>(G[0], G[1], G[2], Nd * nband, ui, c->stream));
+    }
+    const int na = c->has_nl ? c->nl.n_atom : 0;
+    LYNX_TRY(c->fwork.ensure(sizeof(double) * (7 * (size_t)nband + 18 * (size_t)na + (size_t)na + 8)));
+    double* ddot = c->fwork.as<double>();  // [6][nband]
+    double* docc = ddot + 6 * nband;
+    double* dres = docc + nband;           // [6][na][3]
+    double* dea = dres + 18 * na;
+    LYNX_TRY(launch_dot6<T>(G[0], G[1], G[2], Nd, Nd, nband, ddot, c->stream));
+    std::vector<double> dots(6 * (size_t)nband);
+    LYNX_CUDA_TRY(cudaMemcpyAsync(dots.data(), ddot, sizeof(double) * dots.size(), cudaMemcpyDeviceToHost, c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < 6; ++v) {
+        double sum = 0.0;
+        for (int n = 0; n < nband; ++n) sum += occ[n] * dots[(size_t)v * nband + n];
+        stress_k[v] = -of * c->dV * sum;
+        stress_nl[v] = 0.0;
+    }
+    if (!c->has_nl) return LYNX_OK;
+    // chi weighted by the Cartesian position relative to the image centre, per direction
+    const long long totchi = (long long)c->h_chi.size();
+    std::vector<double> wt[3];
+    for (auto& w : wt) w.assign(totchi, 0.0);
+    for (size_t im = 0; im < c->h_img_ndc.size(); ++im) {
+        const int ndc = c->h_img_ndc[im];
+        const int np = c->h_atom_nproj[c->h_img_atom[im]];
+        const long long go = c->h_img_goff[im], co = c->h_img_choff[im];
+        for (int ig = 0; ig < ndc; ++ig) {
+            const int gp = c->h_gpos[go + ig];
+            const int li = gp % c->nx, lj = (gp / c->nx) % c->ny, lk = gp / (c->nx * c->ny);
+            double r[3] = {li * c->dx - img_pos[3 * im], lj * c->dy - img_pos[3 * im + 1],
+                           lk * c->dz - img_pos[3 * im + 2]};
+            if (!c->orth) {
+                const double* u = c->uvec;  // cart_j = sum_i nc_i uvec(i, j)
+                const double a = r[0], b = r[1], e = r[2];
+                for (int j = 0; j < 3; ++j) r[j] = a * u[j] + b * u[3 + j] + e * u[6 + j];
+            }
+            for (int jp = 0; jp < np; ++jp) {
+                const long long k = co + (long long)jp * ndc + ig;
+                for (int b = 0; b < 3; ++b) wt[b][k] = c->h_chi[k] * r[b];
+            }
+        }
+    }
+    for (int b = 0; b < 3; ++b) {
+        LYNX_TRY(c->sbuf[1 + b].ensure(sizeof(double) * std::max<long long>(totchi, 2)));
+        LYNX_CUDA_TRY(cudaMemcpyAsync(c->sbuf[1 + b].p, wt[b].data(), sizeof(double) * totchi, cudaMemcpyHostToDevice,
+                                      c->stream));
+    }
+    const int ncolp = ((nband + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
+    const size_t ab = sizeof(T) * (size_t)c->nl.total_proj * ncolp;
+    LYNX_TRY(c->alpha.ensure(ab));
+    LYNX_TRY(c->fbeta.ensure(ab));
+    const std::vector<double> ones(c->nl.total_proj, 1.0);
+    LYNX_TRY(c->fones.ensure(sizeof(double) * std::max<size_t>(ones.size(), 1)));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(c->fones.p, ones.data(), sizeof(double) * ones.size(), cudaMemcpyHostToDevice,
+                                  c->stream));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(docc, occ, sizeof(double) * nband, cudaMemcpyHostToDevice, c->stream));
+    NLDev raw = c->nl;  // projections without Gamma
+    raw.gamma = c->fones.as<double>();
+    LYNX_TRY(launch_nl_gather<T>(raw, psi, l, nband, c->alpha.as<T>(), ncolp, c->dV, c->stream));
+    static const int va[6] = {0, 0, 0, 1, 1, 2}, vb[6] = {0, 1, 2, 1, 2, 2};
+    for (int v = 0; v < 6; ++v) {
+        NLDev w = raw;
+        w.chi64 = c->sbuf[1 + vb[v]].as<double>();
+        LYNX_TRY(launch_nl_gather<T>(w, G[va[v]], Nd, nband, c->fbeta.as<T>(), ncolp, c->dV, c->stream));
+        // per atom: -2 of sum_n g_n sum_j Gamma Re(conj(alpha) beta); slot v * 3 * na + a * 3 + (v ? 1 : 0);
+        // the energy shares with the first pair
+        LYNX_TRY(launch_nl_force_reduce<T>(c->nl, c->alpha.as<T>(), c->fbeta.as<T>(), ncolp, nband, docc, 2.0 * of, of,
+                                           v ? 1 : 0, dres + (size_t)v * 3 * na, dea, c->stream));
+    }
+    std::vector<double> res(18 * (size_t)na), ea(na);
+    LYNX_CUDA_TRY(cudaMemcpyAsync(res.data(), dres, sizeof(double) * res.size(), cudaMemcpyDeviceToHost, c->stream));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(ea.data(), dea, sizeof(double) * na, cudaMemcpyDeviceToHost, c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    double enl = 0.0;
+    for (int a = 0; a < na; ++a) enl += ea[a];
+    for (int v = 0; v < 6; ++v) {
+        double sum = 0.0;
+        for (int a = 0; a < na; ++a) sum += res[(size_t)v * 3 * na + (size_t)a * 3 + (v ? 1 : 0)];
+        stress_nl[v] = sum - ((v == 0 || v == 3 || v == 5) ? enl : 0.0);
+    }
+    return LYNX_OK;
+}
+
+extern "C" int lynx_kinetic_nonlocal_stress(lynx_ctx* c, const double* psi, int nband, int ld, const double* occ,
+                                            double occfac, const double* img_pos, double* stress_k,
+                                            double* stress_nl) {
+    return stress_impl<double>(c, psi, nband, ld, occ, occfac, img_pos, stress_k, stress_nl, false);
+}
+
+extern "C" int lynx_kinetic_nonlocal_stress_kpt(lynx_ctx* c, const double* psi_z, int nband, int ld,
+                                                const double* occ, double spn_fac_wk, const double* img_pos,
+                                                double* stress_k, double* stress_nl) {
+    return stress_impl<double2>(c, reinterpret_cast<const double2*>(psi_z), nband, ld, occ, 0.5 * spn_fac_wk, img_pos,
+                                stress_k, stress_nl, true);
 }
 
 extern "C" int lynx_eigensolver_solve_batch(lynx_ctx** ctxs, int nb, double** psi, double** eig,

@@ -247,6 +247,99 @@ int launch_grad_dir(int nx, int ny, int nz, int nxp, int R, const double* D1, in
     return LYNX_OK;
 }
 
+struct Mat3Arg {
+    double m[9];
+};
+
+// Cartesian gradients of a non-orthogonal cell from the three lattice-direction gradients, in
+// place: g_a <- sum_d uinv[a][d] g_d (Stress.cpp:1628-1640 and :1188-1200, uinv = uvec^-1).
+template <typename T>
+__global__ void cart_mix_kernel(T* __restrict__ g0, T* __restrict__ g1, T* __restrict__ g2, long long n,
+                                Mat3Arg uinv) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const T a = g0[i], b = g1[i], c = g2[i];
+        T r[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            r[k] = vadd(vadd(vscale(uinv.m[3 * k], a), vscale(uinv.m[3 * k + 1], b)), vscale(uinv.m[3 * k + 2], c));
+        g0[i] = r[0];
+        g1[i] = r[1];
+        g2[i] = r[2];
+    }
+}
+
+template <typename T>
+int launch_cart_mix(T* g0, T* g1, T* g2, long long n, const double* uinv, cudaStream_t st) {
+    Mat3Arg m;
+    for (int k = 0; k < 9; ++k) m.m[k] = uinv[k];
+    cart_mix_kernel<T><<<1184, 256, 0, st>>>(g0, g1, g2, n, m);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("gradient mixing launch failed: %s", cudaGetErrorString(e));
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+__device__ __forceinline__ double re_dot(double a, double b) { return a * b; }
+__device__ __forceinline__ double re_dot(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }
+
+// Six Voigt products of every column, out[v * ncol + n] = sum_i Re(conj(g_a(i, n)) g_b(i, n)),
+// (a, b) = xx, xy, xz, yy, yz, zz.  CTA = one column; each thread sums a fixed strided subset of
+// the points and the block adds the partials in a fixed tree, so the result is reproducible.
+template <typename T>
+__global__ void __launch_bounds__(256) dot6_kernel(const T* __restrict__ g0, const T* __restrict__ g1,
+                                                   const T* __restrict__ g2, long long nd, long long ld,
+                                                   int ncol, double* __restrict__ out) {
+    __shared__ double red[6][256];
+    const int n = blockIdx.x;
+    const T* a0 = g0 + (long long)n * ld;
+    const T* a1 = g1 + (long long)n * ld;
+    const T* a2 = g2 + (long long)n * ld;
+    double s[6] = {0, 0, 0, 0, 0, 0};
+    for (long long i = threadIdx.x; i < nd; i += blockDim.x) {
+        const T x = a0[i], y = a1[i], z = a2[i];
+        s[0] += re_dot(x, x);
+        s[1] += re_dot(x, y);
+        s[2] += re_dot(x, z);
+        s[3] += re_dot(y, y);
+        s[4] += re_dot(y, z);
+        s[5] += re_dot(z, z);
+    }
+#pragma unroll
+    for (int v = 0; v < 6; ++v) red[v][threadIdx.x] = s[v];
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+#pragma unroll
+            for (int v = 0; v < 6; ++v) red[v][threadIdx.x] += red[v][threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) out[(long long)threadIdx.x * ncol + n] = red[threadIdx.x][0];
+}
+
+template <typename T>
+int launch_dot6(const T* g0, const T* g1, const T* g2, long long nd, long long ld, int ncol, double* out,
+                cudaStream_t st) {
+    if (ncol <= 0) return LYNX_OK;
+    dot6_kernel<T><<<ncol, 256, 0, st>>>(g0, g1, g2, nd, ld, ncol, out);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("gradient products launch failed: %s", cudaGetErrorString(e));
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+template int launch_cart_mix<double>(double*, double*, double*, long long, const double*, cudaStream_t);
+template int launch_cart_mix<double2>(double2*, double2*, double2*, long long, const double*, cudaStream_t);
+template int launch_dot6<double>(const double*, const double*, const double*, long long, long long, int, double*,
+                                 cudaStream_t);
+template int launch_dot6<double2>(const double2*, const double2*, const double2*, long long, long long, int, double*,
+                                  cudaStream_t);
+
 template int launch_grad_dir<double>(int, int, int, int, int, const double*, int, const double*, long long, double*,
                                      long long, int, const double*, const double*, cudaStream_t);
 template int launch_grad_dir<double2>(int, int, int, int, int, const double*, int, const double2*, long long, double2*,

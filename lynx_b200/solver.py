@@ -128,6 +128,7 @@ class Context:
                                          tab.n_atom, iptr(npj), dptr(gm)))
         self.has_nonlocal = True
         self.n_atom = int(tab.n_atom)
+        self.img_coords = np.ascontiguousarray(tab.img_coords, dtype=np.float64).reshape(-1, 3)
 
     def set_kpoint(self, kcart):
         k = np.ascontiguousarray(kcart, dtype=np.float64).reshape(3)
@@ -220,6 +221,29 @@ class NonlocalProjector:
             check(ctx.lib.lynx_nonlocal_force(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), a.ncol, ctx.nd, dptr(occ),
                                               occfac * wk, dptr(f), dptr(e)))
         return f[:3 * na].reshape(na, 3), float(e[0])
+
+    def stress(self, psi, occ, occfac: float = 2.0, kpt: bool = False, wk: float = 1.0):
+        """Kinetic and nonlocal stress (Voigt xx, xy, xz, yy, yz, zz) of the orbitals psi with
+        occupations occ, before the division by the cell measure
+        (Hamiltonian::compute_kinetic_nonlocal_stress_gpu / _kpt_gpu; the formula of
+        Stress.cpp:1041-1784).  Returns (stress_k, stress_nl)."""
+        ctx = self.ctx
+        ctx.sync_stream()
+        a = _DeviceArgs(ctx, psi, kpt)
+        occ = np.ascontiguousarray(occ, dtype=np.float64)
+        if occ.shape[0] != a.ncol:
+            raise ValueError("one occupation per orbital column is needed")
+        sk = np.zeros(6)
+        snl = np.zeros(6)
+        pos = getattr(ctx, "img_coords", None) if ctx.has_nonlocal else None
+        pp = dptr(pos) if pos is not None else None
+        if kpt:
+            check(ctx.lib.lynx_kinetic_nonlocal_stress_kpt(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), a.ncol, ctx.nd,
+                                                           dptr(occ), 2.0 * occfac * wk, pp, dptr(sk), dptr(snl)))
+        else:
+            check(ctx.lib.lynx_kinetic_nonlocal_stress(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), a.ncol, ctx.nd,
+                                                       dptr(occ), occfac * wk, pp, dptr(sk), dptr(snl)))
+        return sk, snl
 
 
 class Hamiltonian:

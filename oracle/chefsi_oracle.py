@@ -454,3 +454,77 @@ def nonlocal_force(psi, occ, tab: dict, st, shape, dV, occfac=2.0, wk=1.0, kpt=N
         beta = projections(gradient(psi, shape, st, dim, kpt, lengths), tab, dV, kpt)
         f[:, dim] = -2.0 * occfac * wk * np.sum(occ * gam * np.real(np.conj(alpha) * beta), axis=(1, 2))
     return f, energy
+
+
+# ---------------------------------------------------------------------------
+# Kinetic and nonlocal stress (src/physics/Stress.cpp:1041-1784 compute_nonlocal_kinetic_cpu:
+# real path :1611-1729, k-point path :1229-1400, assembly :1732-1748), returned before the
+# division by the cell measure, as Hamiltonian::compute_kinetic_nonlocal_stress_gpu returns it
+# (src/operators/Hamiltonian.hpp:156-160; src/physics/GPUForce.cu:471-680).
+# ---------------------------------------------------------------------------
+
+VOIGT = ((0, 0), (0, 1), (0, 2), (1, 1), (1, 2), (2, 2))
+
+
+def cartesian_gradients(psi, cell, st, kpt=None):
+    """Cartesian gradients [d/dx, d/dy, d/dz] of psi: lattice-direction FD gradients, mixed by
+    uvec^-1 for non-orthogonal cells (Stress.cpp:1628-1640)."""
+    G = [gradient(psi, cell.shape, st, d, kpt, cell.lengths, tuple(cell.bc)) for d in range(3)]
+    if cell.orthogonal:
+        return G
+    ui = np.linalg.inv(cell.uvec)
+    return [ui[a, 0] * G[0] + ui[a, 1] * G[1] + ui[a, 2] * G[2] for a in range(3)]
+
+
+def weighted_projections(x, tab: dict, cell, dV: float, dim2: int, kpt=None):
+    """beta[atom, jp, n] = dV sum_img e^{-i k.R_img} sum_g chi(g, jp) (r_g - R_img)_dim2 x(g), the
+    relative position taken Cartesian (nonCart2Cart with uvec for non-orthogonal cells;
+    Stress.cpp:1696-1717 real, :1350-1383 k-point)."""
+    x2 = x.reshape(x.shape[0], -1)
+    nproj = int(tab["nproj"])
+    n_atom = len(tab["gamma"]) // nproj if nproj else 0
+    beta = np.zeros((n_atom, nproj, x2.shape[1]), dtype=np.result_type(x2, 1.0))
+    offs = np.concatenate([[0], np.cumsum(tab["img_ndc"])])
+    nx, ny, _ = cell.shape
+    h = cell.spacing
+    uvec = cell.uvec
+    for i in range(len(tab["img_atom"])):
+        ndc = int(tab["img_ndc"][i])
+        chi = np.asarray(tab["chi"][offs[i] * nproj:(offs[i] + ndc) * nproj]).reshape(nproj, ndc).T
+        g = np.asarray(tab["gpos"][offs[i]:offs[i] + ndc])
+        rel = np.stack([(g % nx) * h[0], ((g // nx) % ny) * h[1], (g // (nx * ny)) * h[2]], 1) - tab["img_coords"][i]
+        if not cell.orthogonal:
+            rel = rel @ uvec  # cart_j = sum_i nc_i uvec[i, j]
+        w = rel[:, dim2]
+        fac = dV
+        if kpt is not None:
+            th = -float(np.dot(kpt, tab["img_shift"][i]))
+            fac = complex(math.cos(th), math.sin(th)) * dV
+        beta[tab["img_atom"][i]] += fac * (chi.T @ (w[:, None] * x2[g, :]))
+    return beta
+
+
+def kinetic_nonlocal_stress(psi, occ, tab: dict, st, cell, dV, occfac=2.0, wk=1.0, kpt=None):
+    """(stress_k[6], stress_nl[6]) in Voigt order xx, xy, xz, yy, yz, zz:
+    stress_k = -occfac wk dV sum_n g_n Re <D_a psi_n, D_b psi_n>;
+    stress_nl = -2 occfac wk sum_n g_n sum_jp Gamma Re(conj(alpha) beta_ab) - delta_ab E_nl,
+    E_nl = occfac wk sum_n g_n sum_jp Gamma |alpha|^2."""
+    occ = np.asarray(occ, dtype=np.float64)
+    C = cartesian_gradients(psi, cell, st, kpt)
+    sk = np.zeros(6)
+    for v, (a, b) in enumerate(VOIGT):
+        dots = np.real(np.sum(np.conj(C[a].reshape(C[a].shape[0], -1)) * C[b].reshape(C[b].shape[0], -1), axis=0))
+        sk[v] = -occfac * wk * dV * float(np.sum(occ * dots))
+    snl = np.zeros(6)
+    energy = 0.0
+    if tab is not None and len(tab["img_atom"]):
+        nproj = int(tab["nproj"])
+        gam = np.asarray(tab["gamma"]).reshape(-1, nproj)[:, :, None]
+        oc = occ[None, None, :]
+        alpha = projections(psi, tab, dV, kpt)
+        energy = occfac * wk * float(np.sum(oc * gam * np.abs(alpha) ** 2))
+        for v, (a, b) in enumerate(VOIGT):
+            beta = weighted_projections(C[a], tab, cell, dV, b, kpt)
+            snl[v] = -2.0 * occfac * wk * float(np.sum(oc * gam * np.real(np.conj(alpha) * beta)))
+    snl[[0, 3, 5]] -= energy
+    return sk, snl, energy
