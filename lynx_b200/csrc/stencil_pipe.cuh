@@ -140,6 +140,41 @@ __device__ __forceinline__ void fence_mbar_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Shared-memory loads at 32-bit shared-window addresses.  The consumers keep per-thread byte
+// offsets and advance them by additions; written through generic pointers, every neighbour
+// address cost 64-bit pointer arithmetic, and the integer work outweighed the floating point.
+template <typename V> __device__ __forceinline__ V lds(uint32_t a);
+template <> __device__ __forceinline__ float lds<float>(uint32_t a) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+    return v;
+}
+template <> __device__ __forceinline__ double lds<double>(uint32_t a) {
+    double v;
+    asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"(a));
+    return v;
+}
+template <> __device__ __forceinline__ float2 lds<float2>(uint32_t a) {
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    return v;
+}
+template <> __device__ __forceinline__ double2 lds<double2>(uint32_t a) {
+    double2 v;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a));
+    return v;
+}
+template <> __device__ __forceinline__ int2 lds<int2>(uint32_t a) {
+    int2 v;
+    asm volatile("ld.shared.v2.s32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(a));
+    return v;
+}
+template <> __device__ __forceinline__ int lds<int>(uint32_t a) {
+    int v;
+    asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -401,16 +436,29 @@ __global__ void __launch_bounds__(MAXT, 1)
     for (int k = 0; k < W; ++k) load_own_plane(z0 - R + k, w[k]);
 
     // Entering plane of the window (plane z+R+1 after sub-step i), from the window ring.
+    // Per-thread byte offsets in the staged rows (pitch nxp): rowb per row, yoffb to the
+    // thread's first point in row yl[0] of a block of own rows, soffb the same for the Veff
+    // rows (scalar type S), xcolb the thread's x-neighbour vectors; othr: the thread's first
+    // output point of the chunk's first plane.
+    const uint32_t rowb = (uint32_t)(nxp * (int)sizeof(T));
+    const uint32_t rowbS = (uint32_t)(nxp * (int)sizeof(S));
+    const uint32_t yoffb = (uint32_t)((yl[0] * nxp + xb) * (int)sizeof(T));
+    const uint32_t soffb = (uint32_t)((yl[0] * nxp + xb) * (int)sizeof(S));
+    uint32_t xcolb[NXV];
+#pragma unroll
+    for (int k = 0; k < NXV; ++k) xcolb[k] = (uint32_t)(xcol[k] * (int)sizeof(T));
+    T* const othr = oc + (long long)z0 * G.plane + (long long)(y0 + yl[0]) * nxp + xb;
+
     auto window_entry = [&](int i, int z, VT* dst) -> bool {
         const int wst = i % DW;
         if (!mbar_wait(&wfull[wst], (uint32_t)((i / DW) & 1))) return false;
-        const T* wsrc = wstage_of(wst);
+        const uint32_t wsrc = smem_u32(wstage_of(wst)) + yoffb;
         const bool wrapped = (z + R + 1) >= nz;
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
             VT t;
             if (own[r]) {
-                t = *reinterpret_cast<const VT*>(wsrc + yl[r] * nxp + xb);
+                t = lds<VT>(wsrc + r * rowb);
                 if (wrapped) {
                     T* tp = reinterpret_cast<T*>(&t);
 #pragma unroll
@@ -436,6 +484,13 @@ __global__ void __launch_bounds__(MAXT, 1)
         if constexpr (kPacked) {
             constexpr int J = decltype(Jc)::value;
             float2 acc[RY];
+            // fused nonlocal term: this plane's point map at the thread's first row and the staged
+            // W range, shifted so that a compact point number indexes it directly
+            uint32_t nl_pm = 0, nl_w = 0;
+            if constexpr (NLF) {
+                nl_pm = smem_u32(pm_of(st)) + (uint32_t)((yl[0] * NL.mp + xb) * 4);
+                nl_w = smem_u32(wnl_of(st)) - (uint32_t)walign[st] * 4u;
+            }
             const float2 dg = make_float2(C.diag, C.diag);
 #pragma unroll
             for (int r = 0; r < RY; ++r) {
@@ -446,10 +501,11 @@ __global__ void __launch_bounds__(MAXT, 1)
                                         acc[r]);
             }
             {
-                const float* tcol = tile + (R + yl[0]) * nxp + xb;
+                uint32_t ya = smem_u32(tile) + yoffb;  // row R + yl[0] + q for q = -R
 #pragma unroll
                 for (int q = -R; q < RY + R; ++q) {
-                    float2 v = *reinterpret_cast<const float2*>(tcol + q * nxp);
+                    float2 v = lds<float2>(ya);
+                    ya += rowb;
                     if (PHASED) {
                         if (ywrap_l & (1u << (q + R))) {
                             v.x *= C.phl[1];
@@ -469,11 +525,11 @@ __global__ void __launch_bounds__(MAXT, 1)
 #pragma unroll
             for (int r = 0; r < RY; ++r) {
                 if (!own[r]) continue;
-                const float* trow = tile + (R + yl[r]) * nxp;
+                const uint32_t ra = smem_u32(tile) + (uint32_t)(R + yl[r]) * rowb;
                 float2 P[NXV];
 #pragma unroll
                 for (int k = 0; k < NXV; ++k) {
-                    float2 t = *reinterpret_cast<const float2*>(trow + xcol[k]);
+                    float2 t = lds<float2>(ra + xcolb[k]);
                     if (PHASED) {
                         if (xwrap & (1u << (2 * k))) {
                             t.x *= C.phl[0];
@@ -497,22 +553,20 @@ __global__ void __launch_bounds__(MAXT, 1)
                         acc[r].y = fmaf(C.cx[p], sr.x, acc[r].y);
                     }
                 }
-                const int so = yl[r] * nxp + xb;
-                const float2 vv = *reinterpret_cast<const float2*>(v_s + so);
+                const float2 vv = lds<float2>(smem_u32(v_s) + soffb + r * rowbS);
                 acc[r] = __ffma2_rn(__fmul2_rn(make_float2(C.a, C.a), vv), w[J + R][r], acc[r]);
-                if (XOLD) acc[r] = __ffma2_rn(make_float2(C.d, C.d), *reinterpret_cast<const float2*>(xo_s + so), acc[r]);
+                if (XOLD) acc[r] = __ffma2_rn(make_float2(C.d, C.d), lds<float2>(smem_u32(xo_s) + yoffb + r * rowb), acc[r]);
                 if constexpr (NLF) {
-                    const int2 m = *reinterpret_cast<const int2*>(pm_of(st) + yl[r] * NL.mp + xb);
-                    const float* wn = wnl_of(st) - walign[st];
-                    if (m.x >= 0) acc[r].x = fmaf(C.a, wn[m.x], acc[r].x);
-                    if (m.y >= 0) acc[r].y = fmaf(C.a, wn[m.y], acc[r].y);
+                    const int2 m = lds<int2>(nl_pm + (uint32_t)r * (uint32_t)(NL.mp * 4));
+                    if (m.x >= 0) acc[r].x = fmaf(C.a, lds<float>(nl_w + (uint32_t)m.x * 4u), acc[r].x);
+                    if (m.y >= 0) acc[r].y = fmaf(C.a, lds<float>(nl_w + (uint32_t)m.y * 4u), acc[r].y);
                     if (NL.xs_out) {
                         float* xs = NL.xs_out + col * NL.ldw;
                         if (m.x >= 0) xs[m.x] = acc[r].x;
                         if (m.y >= 0) xs[m.y] = acc[r].y;
                     }
                 }
-                float* op = oc + (long long)z * G.plane + (long long)(y0 + yl[r]) * nxp + xb;
+                float* op = othr + (long long)(z - z0) * G.plane + r * nxp;
                 *reinterpret_cast<float2*>(op) = acc[r];
             }
         }
@@ -547,10 +601,11 @@ __global__ void __launch_bounds__(MAXT, 1)
         }
         // y neighbours: each staged row is read once and feeds every row within R of it
         {
-            const T* tcol = tile + (R + yl[0]) * nxp + xb;
+            uint32_t ya = smem_u32(tile) + yoffb;  // row R + yl[0] + q for q = -R
 #pragma unroll
             for (int q = -R; q < RY + R; ++q) {
-                VT v = *reinterpret_cast<const VT*>(tcol + q * nxp);
+                VT v = lds<VT>(ya);
+                ya += rowb;
                 T* ve = reinterpret_cast<T*>(&v);
                 if (PHASED) {
                     if (ywrap_l & (1u << (q + R))) {
@@ -574,13 +629,13 @@ __global__ void __launch_bounds__(MAXT, 1)
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
             if (!own[r]) continue;
-            const T* trow = tile + (R + yl[r]) * nxp;
+            const uint32_t ra = smem_u32(tile) + (uint32_t)(R + yl[r]) * rowb;
             // x neighbours
             {
                 T xv[NXV * RX];
 #pragma unroll
                 for (int k = 0; k < NXV; ++k) {
-                    VT t = *reinterpret_cast<const VT*>(trow + xcol[k]);
+                    VT t = lds<VT>(ra + xcolb[k]);
                     if (PHASED) {
                         T* tp = reinterpret_cast<T*>(&t);
                         if (xwrap & (1u << (2 * k))) {
@@ -599,18 +654,18 @@ __global__ void __launch_bounds__(MAXT, 1)
                     for (int p = 1; p <= R; ++p)
                         acc[r][u] = fmac(acc[r][u], C.cx[p], vadd(xv[XOFF + u + p], xv[XOFF + u - p]));
             }
-            const int so = yl[r] * nxp + xb;
             const T* wc = reinterpret_cast<const T*>(&w[J + R][r]);
             {
                 S vv[RX];
+                const uint32_t va = smem_u32(v_s) + soffb + r * rowbS;
                 if constexpr (RX == 2) {
                     using SV = typename VecOf<S, 2>::type;
-                    *reinterpret_cast<SV*>(vv) = *reinterpret_cast<const SV*>(v_s + so);
+                    *reinterpret_cast<SV*>(vv) = lds<SV>(va);
                 } else {
-                    vv[0] = v_s[so];
+                    vv[0] = lds<S>(va);
                 }
                 VT xo_v;
-                if (XOLD) xo_v = *reinterpret_cast<const VT*>(xo_s + so);
+                if (XOLD) xo_v = lds<VT>(smem_u32(xo_s) + yoffb + r * rowb);
                 const T* xo_e = reinterpret_cast<const T*>(&xo_v);
 #pragma unroll
                 for (int u = 0; u < RX; ++u) {
@@ -630,7 +685,7 @@ __global__ void __launch_bounds__(MAXT, 1)
                     }
                 }
             }
-            T* op = oc + (long long)z * G.plane + (long long)(y0 + yl[r]) * nxp + xb;
+            T* op = othr + (long long)(z - z0) * G.plane + r * nxp;
             VT o;
             T* opv = reinterpret_cast<T*>(&o);
 #pragma unroll
