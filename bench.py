@@ -34,10 +34,10 @@ METRIC = "s/SCF-iter Si216 CheFSI: mixed vs plain FP64 on B200 at ΔE≤1e-5 Ha/
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one cheb_pipe_kernel launch per
 # grid-point x state update, from an ncu capture of the Si64 case (60^3 grid, 160 states, the
-# launch shape the autotuner picks there): 446.7 MB (FP32) and 864.1 MB (FP64) per launch.
+# launch shape the autotuner picks there): 440.3 MB (FP32) and 864.1 MB (FP64) per launch.
 # Whole planes stream through the same band geometry at every size, so the traffic of a launch
 # scales with the updates it processes.
-TRAFFIC_PER_UPDATE = {"mixed": 446.657e6 / (216000 * 160), "fp64": 864.076e6 / (216000 * 160)}
+TRAFFIC_PER_UPDATE = {"mixed": 440.271e6 / (216000 * 160), "fp64": 864.076e6 / (216000 * 160)}
 
 CONFIGS = {
     # name: (reps, grid, nstates, degree, displace)

@@ -36,7 +36,7 @@
 namespace lynxb {
 
 constexpr int kPipeMaxThreads = 352;
-constexpr long long kSpinLimit = 1LL << 22;  // bounded mbarrier waits
+constexpr int kSpinLimit = 1 << 22;  // bounded mbarrier waits (a 32-bit counter: cheaper per wait)
 
 struct PipeGeom {
     int nx, ny, nz;
@@ -110,7 +110,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 // Bounded wait for the phase with the given parity; returns false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     const uint32_t addr = smem_u32(bar);
-    for (long long i = 0; i < kSpinLimit; ++i) {
+    for (int i = 0; i < kSpinLimit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
