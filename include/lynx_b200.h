@@ -195,6 +195,15 @@ LYNX_API int lynx_nonlocal_force(lynx_ctx* ctx, const double* psi, int nband, in
 LYNX_API int lynx_nonlocal_force_kpt(lynx_ctx* ctx, const double* psi_z, int nband, int ld, const double* occ,
                                      double spn_fac_wk, double* force, double* energy_nl);
 
+/* Start orbitals on the device, as the reference's GPU path draws them: a cuRAND default
+ * pseudo-random generator (XORWOW) seeded with `seed` fills nband contiguous columns of Nd
+ * doubles (2 Nd for complex, real and imaginary interleaved) with uniform values in (0, 1].
+ * The reference seeds (spin s, k-point k) with (spin_start + s) * 1000 + (s * Nkpts + k) * 13 + 1.
+ * ld must be Nd or 0.  Replaces EigenSolver::randomize_psi_gpu (src/solvers/EigenSolver.hpp:160;
+ * src/solvers/EigenSolver.cu:1199-1228) for one (spin, k-point) block. */
+LYNX_API int lynx_randomize_orbitals(lynx_ctx* ctx, double* psi, int nband, int ld, unsigned long long seed,
+                                     int is_complex);
+
 /* Kinetic and nonlocal stress of device psi (nband columns, leading dimension ld), before the
  * division by the cell measure, Voigt order xx, xy, xz, yy, yz, zz:
  *   stress_k[ab]  = -occfac dV sum_n occ[n] <D_a psi_n, D_b psi_n>,

@@ -12,6 +12,7 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
+#include <curand.h>
 
 #include <algorithm>
 #include <array>
@@ -2151,6 +2152,29 @@ extern "C" int lynx_kinetic_nonlocal_stress_kpt(lynx_ctx* c, const double* psi_z
                                                 double* stress_k, double* stress_nl) {
     return stress_impl<double2>(c, reinterpret_cast<const double2*>(psi_z), nband, ld, occ, 0.5 * spn_fac_wk, img_pos,
                                 stress_k, stress_nl, true);
+}
+
+extern "C" int lynx_randomize_orbitals(lynx_ctx* c, double* psi, int nband, int ld, unsigned long long seed,
+                                       int is_complex) {
+    LYNX_CHECK_ARG(c && psi, "null pointer");
+    LYNX_CHECK_ARG(nband > 0, "nband must be positive");
+    LYNX_CHECK_ARG(ld == 0 || ld == c->Nd, "the start orbitals fill contiguous columns: ld must be Nd (or 0)");
+    LYNX_TRY(activate(c));
+    curandGenerator_t g = nullptr;
+    if (curandCreateGenerator(&g, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS) {
+        set_error("curandCreateGenerator failed");
+        return LYNX_ERR_CUDA;
+    }
+    const size_t n = (size_t)c->Nd * nband * (is_complex ? 2 : 1);
+    curandStatus_t r = curandSetStream(g, c->stream);
+    if (r == CURAND_STATUS_SUCCESS) r = curandSetPseudoRandomGeneratorSeed(g, seed);
+    if (r == CURAND_STATUS_SUCCESS) r = curandGenerateUniformDouble(g, psi, n);
+    curandDestroyGenerator(g);
+    if (r != CURAND_STATUS_SUCCESS) {
+        set_error("cuRAND uniform generation failed (status %d)", (int)r);
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
 }
 
 extern "C" int lynx_eigensolver_solve_batch(lynx_ctx** ctxs, int nb, double** psi, double** eig,

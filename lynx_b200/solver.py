@@ -371,6 +371,18 @@ def occupations(eigs, ef: float, beta: float, smearing: str = "fermi-dirac") -> 
     return occ
 
 
+def randomize_orbitals(ctx: Context, nband: int, seed: int, complex_: bool = False):
+    """Device start orbitals as EigenSolver::randomize_psi_gpu draws them (cuRAND default
+    generator, uniform (0, 1], seed as given): a torch tensor (nband, Nd), float64 or complex128
+    (real and imaginary parts interleaved, as the generator fills them)."""
+    torch = _torch()
+    ctx.sync_stream()
+    t = torch.empty((nband, ctx.nd * (2 if complex_ else 1)), dtype=torch.float64, device=f"cuda:{ctx.device}")
+    check(ctx.lib.lynx_randomize_orbitals(ctx.handle, ctypes.c_void_p(t.data_ptr()), int(nband), ctx.nd,
+                                          ctypes.c_ulonglong(int(seed)), 1 if complex_ else 0))
+    return torch.view_as_complex(t.view(nband, ctx.nd, 2)) if complex_ else t
+
+
 def solve_batch(solvers, psis, Veffs, lambda_cutoffs, eigval_mins, eigval_maxs, cheb_degree: int = 20,
                 precision: Optional[str] = None, kpt=False):
     """One CheFSI pass of several independent problems at once (lynx_eigensolver_solve_batch).
