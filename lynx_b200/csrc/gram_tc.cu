@@ -45,6 +45,9 @@ constexpr int NSLICE = 3;
 constexpr int TILE_BYTES = BM * BK;                      // 16 KB, one slice tile
 constexpr int STAGE_BYTES = 2 * NSLICE * TILE_BYTES;     // A and B slices: 96 KB
 constexpr int TMEM_COLS = 512;                           // 3 accumulators x 128 columns, power of two
+// Rotation: the epilogue splits each TMEM lane quarter's 128 columns into kRotParts parts, one
+// warp each (kRotParts * 4 warps; BN / kRotParts a multiple of 16).
+constexpr int kRotParts = 4, kRotThreads = 128 * kRotParts;
 constexpr int kMaxChunkSteps = 1365;  // 3 * 64 * 64 * 128 * 1365 < 2^31: int32 accumulators cannot overflow
 // kind::i8 instruction descriptor: D = S32 (bits 4-5 = 2), A = B = signed 8-bit (bits 7-9,
 // 10-12 = 1), K-major A and B, N>>3 at bits 17-22, M>>4 at bits 24-28.
@@ -459,7 +462,7 @@ struct RotArgs {
     int* err;
 };
 
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kRotThreads, 1)
     rot_i8_kernel(const __grid_constant__ CUtensorMap tA1, const __grid_constant__ CUtensorMap tA2,
                   const __grid_constant__ CUtensorMap tA3, const __grid_constant__ CUtensorMap tB1,
                   const __grid_constant__ CUtensorMap tB2, const __grid_constant__ CUtensorMap tB3,
@@ -548,8 +551,14 @@ __global__ void __launch_bounds__(128, 1)
     if (!mbar_wait(done, 0)) ok = false;
     ok = __all_sync(0xffffffffu, ok);
     tc_fence_after();
+    // Epilogue on all warps: warp w reads TMEM lane quarter w % 4 (its 32 rows) and the column
+    // part w / 4 of kRotParts, so the stores of several warps per quarter are in flight.
+    __shared__ double fps[BN];  // column scales of this tile
+    if (threadIdx.x < BN) fps[threadIdx.x] = (n0 + (int)threadIdx.x < g.N) ? g.fpow[n0 + threadIdx.x] : 0.0;
+    __syncthreads();
     if (ok) {
-        const long long row = (long long)m0 + warp * 32 + lane;
+        const int quarter = warp & 3, part = warp >> 2;
+        const long long row = (long long)m0 + quarter * 32 + lane;
         long long ridx = -1;
         double rs = 1.0;
         if (row < g.rows) {
@@ -557,9 +566,9 @@ __global__ void __launch_bounds__(128, 1)
             if (xr < g.nx) ridx = xr + (long long)g.nx * rest;
             rs = pow2d(g.erow[row]);
         }
-        const uint32_t lb = (uint32_t)(warp * 32) << 16;
+        const uint32_t lb = (uint32_t)(quarter * 32) << 16;
 #pragma unroll 1
-        for (int c0 = 0; c0 < BN; c0 += 16) {
+        for (int c0 = part * (BN / kRotParts); c0 < (part + 1) * (BN / kRotParts); c0 += 16) {
             uint32_t r2[16], r3[16], r4[16];
             tmem_ld16(tmem + lb + (uint32_t)c0, r2);
             tmem_ld16(tmem + lb + 128u + (uint32_t)c0, r3);
@@ -572,7 +581,7 @@ __global__ void __launch_bounds__(128, 1)
                     if (j < g.N) {
                         const double x = (double)(int)r2[t] * 0x1p-14 + (double)(int)r3[t] * 0x1p-21 +
                                          (double)(int)r4[t] * 0x1p-28;
-                        g.psi[(long long)j * g.ldp + ridx] = x * rs * g.fpow[j];  // exact: powers of two
+                        g.psi[(long long)j * g.ldp + ridx] = x * rs * fps[c0 + t];  // exact: powers of two
                     }
                 }
             }
@@ -802,7 +811,7 @@ int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp
     const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
     LYNX_CUDA_TRY(smem_cap(rot_i8_kernel, smem));
     const long long ntm = (rows + BM - 1) / BM;
-    rot_i8_kernel<<<(unsigned)(ntm * g.ntn), 128, smem, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], g);
+    rot_i8_kernel<<<(unsigned)(ntm * g.ntn), kRotThreads, smem, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], g);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
