@@ -78,6 +78,9 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--profile-pass", action="store_true",
+                   help="bracket the first timed pass with cudaProfilerStart/Stop, so that "
+                        "`ncu --profile-from-start off` captures exactly one pass")
     return p.parse_args()
 
 
@@ -303,15 +306,20 @@ def main():
            "band_energy_dE_per_atom_Ha": float(abs(2.0 * (eig_mixed[:nocc] - eig_fp64[:nocc]).sum()) / natom)}
 
     # FP64 timing (the plain-FP64 GPU CheFSI the mixed path is compared against)
-    def timed(precision, k):
+    def timed(precision, k, profile=False):
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        for _ in range(k):
+        for i in range(k):
+            if profile and i == 0:
+                torch.cuda.profiler.start()
             one_pass(precision)
+            if profile and i == 0:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.stop()
         e1.record()
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / k
@@ -321,7 +329,7 @@ def main():
 
     lib.lynx_launch_count(1)
     with ClockSampler(local) as clk:
-        t_main = timed(args.precision, args.steps)
+        t_main = timed(args.precision, args.steps, args.profile_pass)
     launches = int(lib.lynx_launch_count(1))
     t_main = max_over_ranks(t_main, world, "cuda")
 
