@@ -440,28 +440,28 @@ int ensure_layout(lynx_ctx* c, DevBuf& b, size_t bytes, int tag) {
 
 // Copy/convert the valid points of ncol columns between row layouts (row length nxp, column stride ld).
 template <typename Dst, typename Src>
-__global__ void repack_kernel(Dst* __restrict__ dst, int dnxp, long long dld, const Src* __restrict__ src, int snxp,
-                              long long sld, int nx, long long nrows, int ncol) {
-    const long long per_col = (long long)nx * nrows;
-    const long long total = per_col * ncol;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        const long long cidx = i / per_col;
-        const long long rem = i - cidx * per_col;
-        const long long r = rem / nx;
-        const int xi = (int)(rem - r * nx);
-        cvt_val(dst[cidx * dld + r * dnxp + xi], src[cidx * sld + r * snxp + xi]);
-    }
+__global__ void __launch_bounds__(256) repack_kernel(Dst* __restrict__ dst, int dnxp, long long dld,
+                                                     const Src* __restrict__ src, int snxp, long long sld, int nx,
+                                                     long long nrows) {
+    // one warp per grid row (lanes along x), eight rows per CTA, blockIdx.y = column
+    const long long r = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (r >= nrows) return;
+    const Src* s = src + (long long)blockIdx.y * sld + r * snxp;
+    Dst* d = dst + (long long)blockIdx.y * dld + r * dnxp;
+    for (int xi = threadIdx.x & 31; xi < nx; xi += 32) cvt_val(d[xi], s[xi]);
 }
 
 template <typename Dst, typename Src>
 int repack(lynx_ctx* c, Dst* dst, int dnxp, long long dld, const Src* src, int snxp, long long sld, int ncol) {
-    const long long total = (long long)c->nx * c->ny * c->nz * ncol;
-    if (total == 0) return LYNX_OK;
-    const int blocks = (int)std::min<long long>((total + 255) / 256, 148LL * 16);
-    repack_kernel<Dst, Src><<<blocks, 256, 0, c->stream>>>(dst, dnxp, dld, src, snxp, sld, c->nx,
-                                                           (long long)c->ny * c->nz, ncol);
-    count_launch();
+    const long long nrows = (long long)c->ny * c->nz;
+    if (nrows == 0 || ncol <= 0) return LYNX_OK;
+    for (int c0 = 0; c0 < ncol; c0 += 65535) {  // grid.y limit
+        const int nc = std::min(65535, ncol - c0);
+        dim3 grid((unsigned)((nrows + 7) / 8), (unsigned)nc);
+        repack_kernel<Dst, Src><<<grid, 256, 0, c->stream>>>(dst + (long long)c0 * dld, dnxp, dld,
+                                                             src + (long long)c0 * sld, snxp, sld, c->nx, nrows);
+        count_launch();
+    }
     LYNX_CUDA_TRY(cudaGetLastError());
     return LYNX_OK;
 }
