@@ -31,6 +31,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "s/SCF-iter Si216 CheFSI: mixed vs plain FP64 on B200 at ΔE≤1e-5 Ha/atom; HBM GB/s"
+METRIC_NOTE = ("value = seconds per CheFSI pass at fixed V_eff (filter + H*Y + Rayleigh-Ritz), the "
+               "eigensolver part of an SCF iteration; XC, Poisson and mixing are outside this path")
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one cheb_pipe_kernel launch per
 # grid-point x state update, from an ncu capture of the Si64 case (60^3 grid, 160 states, the
@@ -38,6 +40,8 @@ METRIC = "s/SCF-iter Si216 CheFSI: mixed vs plain FP64 on B200 at ΔE≤1e-5 Ha/
 # Whole planes stream through the same band geometry at every size, so the traffic of a launch
 # scales with the updates it processes.
 TRAFFIC_PER_UPDATE = {"mixed": 440.271e6 / (216000 * 160), "fp64": 864.076e6 / (216000 * 160)}
+# The same for the launch the pass runs, with the fused nonlocal term (filled from its capture).
+TRAFFIC_PER_UPDATE_FUSED = {"mixed": None, "fp64": None}
 
 CONFIGS = {
     # name: (reps, grid, nstates, degree, displace)
@@ -51,6 +55,58 @@ CONFIGS = {
 # CheFSI pass over all 68 problems.
 BATCH_CONFIG = "kpt_ensemble"
 BATCH_METRIC = "s per CheFSI pass over a batch: Si2 FCC 4x4x4 k-points + 32 strained Si8 cells"
+
+
+def workload_config(config, cl, nst, degree, natom, world):
+    """The `config` dict of both arms (the same workload for the GPU arm and the reference arm)."""
+    from lynx_b200 import cell as C
+    return {"workload": f"{config} CheFSI pass at fixed V_eff", "grid": cl.shape[0], "nstates": nst,
+            "degree": degree, "fd_order": 12, "natom": natom,
+            "parallelism": "replicas" if world > 1 else "single",
+            "l2": "inputs larger than L2 (FP32 orbital blocks of %.2f GB)" % (4 * cl.nd * nst / 1e9)}
+
+
+def converged_accuracy(solver, ctx, es, psi, Vd, lc, emin, hi, degree, nocc, natom, max_passes=60):
+    """Mixed vs FP64 at convergence (see main).  Leaves psi as it found it."""
+    import torch
+    start = psi.clone()
+    out = {}
+    npass = None
+    for prec in ("fp64", "mixed"):
+        psi.copy_(start)
+        l, e = lc, emin
+        prev, last = None, None
+        n = 0
+        while True:
+            _, eig = es.solve(psi, Vd, l, e, hi, degree, precision=prec)
+            eig = np.asarray(eig).copy()
+            l, e = es.lambda_cutoff(), float(eig[0])
+            n += 1
+            if prev is not None:
+                last = float(np.abs(eig[:nocc] - prev[:nocc]).max())
+            prev = eig
+            if prec == "fp64" and ((last is not None and last < 1e-9) or n >= max_passes):
+                npass = n
+                break
+            if prec == "mixed" and n >= npass:
+                break
+        nel = 4.0 * natom
+        ef = solver.fermi_level(eig, 2.0 * np.ones(len(eig)), nel, 1000.0)
+        occ = solver.occupations(eig, ef, 1000.0)
+        f, _ = solver.NonlocalProjector(ctx).force(psi, occ, occfac=2.0)
+        out[prec] = (eig, np.asarray(f), last)
+    psi.copy_(start)
+    torch.cuda.synchronize()
+    e64, f64, last64 = out["fp64"]
+    em, fm, _ = out["mixed"]
+    return {"passes": npass, "fp64_last_change_occ_Ha": last64,
+            "max_abs_dE_occ_Ha": float(np.abs(em[:nocc] - e64[:nocc]).max()),
+            "band_energy_dE_per_atom_Ha": float(abs(2.0 * (em[:nocc] - e64[:nocc]).sum()) / natom),
+            "max_abs_dF_nonlocal_Ha_per_Bohr": float(np.abs(fm - f64).max()),
+            "max_abs_F_nonlocal_Ha_per_Bohr": float(np.abs(f64).max()),
+            "how": "FP64 passes from the state after the timed passes until the occupied Ritz values move "
+                   "< 1e-9 Ha, the same number of mixed passes from the same state; forces: nonlocal, "
+                   "Fermi-Dirac occupations at 0.001 Ha"}
 
 
 def replica_seed(rank: int) -> int:
@@ -98,23 +154,9 @@ def build_system(config, seed=2024):
 
 
 def veff_separable(cl, pos, depth=1.2, width=1.1, noise=0.0, seed=0):
-    """Same potential as lynx_b200.cell.synthetic_veff for orthogonal cells, evaluated
-    separably (sum over atoms of products of periodic 1-D Gaussians)."""
-    nx, ny, nz = cl.shape
-    h = cl.spacing
-    L = cl.lengths
-    axes = [np.arange(n) * h[d] for d, n in enumerate((nx, ny, nz))]
-    V = np.zeros((nz, ny, nx))
-    for p in pos:
-        g = []
-        for d in range(3):
-            x = axes[d][:, None] - p[d] - L[d] * np.arange(-2, 3)[None, :]
-            g.append(np.exp(-x * x / (2 * width * width)).sum(1))
-        V -= depth * np.einsum("k,j,i->kji", g[2], g[1], g[0])
-    V = V.ravel()
-    if noise > 0:
-        V += np.random.default_rng(seed).normal(0.0, noise, size=V.shape)
-    return V
+    """The synthetic potential of lynx_b200.cell.synthetic_veff, evaluated separably."""
+    from lynx_b200 import cell as C
+    return C.synthetic_veff_separable(cl, pos, depth=depth, width=width, noise=noise, seed=seed)
 
 
 class ClockSampler:
@@ -224,6 +266,28 @@ def cpu_baseline_sample(cl, pos, psp_path, V, nstates, degree, cols=8):
     return total, nthreads, sample, {"filter_s": t_filter, "rr_s": t_rr}
 
 
+def sample_check(psp_path):
+    """The sampled estimate of cpu_baseline_sample checked against one whole reference pass, at
+    the Si64 workload (60^3 grid, 160 states, degree 20), where a whole pass takes seconds:
+    returns both times and their ratio."""
+    from lynx_b200 import cell as C
+    from oracle import ref
+    reps, grid, nst, degree, disp = CONFIGS["si64"]
+    cl, pos = C.diamond_si(reps, grid, displace=disp, seed=2024)
+    V = veff_separable(cl, pos, noise=1e-3, seed=2024)
+    est, cores, _, _ = cpu_baseline_sample(cl, pos, psp_path, V, nst, degree)
+    ref.set_threads(cores)
+    R = ref.RefLynx(cl, pos, psp_path)
+    lo, hi = R.lanczos(V, maxit=60)
+    X = C.random_orbitals(R.nd, nst, seed=9)
+    t0 = time.perf_counter()
+    R.solve(X, V, 0.5 * (lo + hi), lo, hi, degree)
+    full = time.perf_counter() - t0
+    ref.lib().ref_free()
+    return {"workload": "si64 CheFSI pass at fixed V_eff (60^3, 160 states, degree 20)", "whole_pass_s": full,
+            "sampled_estimate_s": est, "whole_over_estimate": full / est, "cores": cores}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -239,14 +303,15 @@ def run_reference(args, rank, world):
             times.append(t)
     v = float(np.mean(times))
     line = {
-        "metric": METRIC, "value": v, "unit": "s/iter", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": f"{args.config} CheFSI pass", "grid": cl.shape[0], "nstates": nst,
-                   "degree": degree, "fd_order": 12, "parallelism": "replicas"},
+        "metric": METRIC, "metric_note": METRIC_NOTE, "value": v, "unit": "s/iter", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": workload_config(args.config, cl, nst, degree, len(pos), world),
         "cpu_baseline": {"value": v, "unit": "s/iter", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": v, "unit": "s/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if args.config != "si64":
+        line["sample_check"] = sample_check(psp_path)
     print(json.dumps(line))
 
 
@@ -290,20 +355,8 @@ def main():
 
     for _ in range(args.warmup):
         one_pass(args.precision)
-    # accuracy check on the warmed-up subspace: one pass in each precision from the same state
-    psi_save = psi.clone()
-    st = (lc, emin)
-    eig_fp64 = one_pass("fp64")
-    psi.copy_(psi_save)
-    lc, emin = st
-    eig_mixed = one_pass("mixed")
-    psi.copy_(psi_save)
-    lc, emin = st
-    del psi_save
     natom = len(pos)
     nocc = 2 * natom  # 4 valence electrons per Si, 2 per state
-    acc = {"max_abs_dE_occ_Ha": float(np.abs(eig_mixed[:nocc] - eig_fp64[:nocc]).max()),
-           "band_energy_dE_per_atom_Ha": float(abs(2.0 * (eig_mixed[:nocc] - eig_fp64[:nocc]).sum()) / natom)}
 
     # FP64 timing (the plain-FP64 GPU CheFSI the mixed path is compared against)
     def timed(precision, k, profile=False):
@@ -333,11 +386,20 @@ def main():
     launches = int(lib.lynx_launch_count(1))
     t_main = max_over_ranks(t_main, world, "cuda")
 
-    # Roofline of the dominant kernel: the fused Chebyshev step, timed alone with CUDA events.
+    # Converged accuracy: from the state after the timed passes, FP64 passes until the occupied
+    # Ritz values stop moving, and the same number of mixed passes from the same state; then the
+    # occupied Ritz values and the nonlocal forces (Fermi-Dirac, 0.001 Ha) of both.  Untimed.
+    acc = converged_accuracy(solver, ctx, es, psi, Vd, lc, emin, hi, degree, nocc, natom)
+
+    # Roofline of the dominant kernel: the stencil kernel as the pass runs it (nonlocal term fused),
+    # each launch timed alone with CUDA events on the context's stream.
     import ctypes
-    ms = ctypes.c_double()
     prec_id = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
     ctx.sync_stream()
+    ms_k = ctypes.c_double()
+    _lib.check(lib.lynx_time_filter_step(ctx.handle, ctypes.c_void_p(Vd.data_ptr()), nst, prec_id, 2, 10,
+                                         ctypes.byref(ms_k)))
+    ms = ctypes.c_double()
     _lib.check(lib.lynx_time_filter_step(ctx.handle, ctypes.c_void_p(Vd.data_ptr()), nst, prec_id, 0, 10,
                                          ctypes.byref(ms)))
     ms_nl = ctypes.c_double()
@@ -345,8 +407,10 @@ def main():
                                          ctypes.byref(ms_nl)))
     wsize = 4 if args.precision == "mixed" else 8
     step_bytes = wsize * ctx.nd * (3 * nst + 1)  # x, xold, out per update + V per point
+    n_pts = int(np.unique(np.asarray(tab.gpos)).size)  # distinct sphere points: the fused term reads
+    fused_bytes = step_bytes + wsize * n_pts * nst   # one (chi alpha) value per sphere point and state
     hbm, bf16, peak_kind = measured_peaks()
-    achieved = step_bytes / (ms.value * 1e-3) / 1e9
+    achieved = fused_bytes / (ms_k.value * 1e-3) / 1e9
     updates = ctx.nd * nst * degree
 
     e2e = None
@@ -381,22 +445,25 @@ def main():
 
     if rank == 0:
         line = {
-            "metric": METRIC, "value": t_main, "unit": "s/iter", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_main * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
-            "config": {"workload": f"{args.config} CheFSI pass ({args.precision})", "grid": cl.shape[0],
-                       "nstates": nst, "degree": degree, "fd_order": 12, "natom": natom,
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (orbital blocks of %.2f GB)" % (wsize * ctx.nd * nst / 1e9)},
+            "metric": METRIC, "metric_note": METRIC_NOTE, "value": t_main, "unit": "s/iter", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_main * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "mixed" else "f64",
+            "data": "synthetic", "config": workload_config(args.config, cl, nst, degree, natom, world),
             "updates_per_s": world * updates / t_main,
             "fp64_s_per_iter" if args.precision == "mixed" else "mixed_s_per_iter": t_other,
             "speedup_vs_fp64" if args.precision == "mixed" else "speedup_vs_mixed": t_other / t_main,
             "accuracy": acc,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": TRAFFIC_PER_UPDATE[args.precision] * ctx.nd * nst,
+                         "traffic": (TRAFFIC_PER_UPDATE_FUSED[args.precision] * ctx.nd * nst
+                                     if TRAFFIC_PER_UPDATE_FUSED[args.precision] else None),
                          "traffic_source": "ncu capture of the Si64 case scaled by updates per launch",
-                         "kernel": "cheb_pipe_kernel (fused stencil + Veff + three-term recurrence)",
-                         "ms_per_launch": ms.value, "ms_per_step_with_nonlocal": ms_nl.value,
+                         "kernel": "cheb_pipe_kernel with the fused nonlocal term (stencil + Veff + a*chi*alpha + "
+                                   "three-term recurrence), as the pass runs it",
+                         "algorithmic_bytes": fused_bytes, "ms_per_launch": ms_k.value,
+                         "plain_step": {"ms_per_launch": ms.value, "algorithmic_bytes": step_bytes,
+                                        "frac": step_bytes / (ms.value * 1e-3) / 1e9 / hbm},
+                         "whole_degree_step": {"ms": ms_nl.value, "frac_of_3_word_floor":
+                                               step_bytes / (ms_nl.value * 1e-3) / 1e9 / hbm},
                          "peak_kind": peak_kind},
             "clocks": clk.summary(),
             "gpu_launches": launches,

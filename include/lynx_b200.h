@@ -50,7 +50,7 @@ enum {
 /* Arithmetic of the CheFSI pass. */
 enum {
     LYNX_PREC_FP64 = 0,  /* plain FP64 everywhere */
-    LYNX_PREC_MIXED = 1  /* FP32 filter + BF16x3 tensor-core Rayleigh-Ritz products, FP64 subspace algebra */
+    LYNX_PREC_MIXED = 1  /* FP32 filter + exact int8-slice tensor-core Rayleigh-Ritz products, FP64 subspace algebra */
 };
 
 enum { LYNX_BC_PERIODIC = 0, LYNX_BC_DIRICHLET = 1 };
@@ -235,11 +235,39 @@ LYNX_API int lynx_fermi_level(const double* eigs, const double* weights, int n, 
 LYNX_API int lynx_occupations(const double* eigs, int n, double ef, double beta, int smearing, double* occ);
 
 /* Diagnostic, no counterpart in the reference: device time of one Chebyshev degree step
- * (out = a*H*x + b*x + d*xold over ncol columns of this context's grid, with or without the
- * nonlocal gather/scatter), averaged over `reps` back-to-back steps on the context's work
- * buffers and timed with CUDA events on the context's stream. */
+ * (out = a*H*x + b*x + d*xold over ncol columns of this context's grid), averaged over `reps`
+ * back-to-back steps on the context's work buffers and timed with CUDA events on the context's
+ * stream.  with_nonlocal: 0 = the local step alone; 1 = the whole step with the nonlocal term
+ * (projections, expansion and stencil); 2 = the same step, but the time returned is that of
+ * the stencil kernel launch alone (the nonlocal term fused into it where it applies), each
+ * launch bracketed by its own events. */
 LYNX_API int lynx_time_filter_step(lynx_ctx* ctx, const double* veff, int ncol, int precision, int with_nonlocal,
                                    int reps, double* ms_per_step);
+
+/* Rayleigh-Ritz products of the mixed-precision pass on FP32 blocks (device pointers, rows x n,
+ * column stride ld; ld and rows multiples of 4, Y and HY 16-byte aligned), on the tensor cores
+ * with exact int8 slices and an FP64 result:
+ *   Ms = scale * Y^T Y  (N x N column-major; only the upper triangle is guaranteed),
+ *   Hs = scale * Y^T HY (N x N column-major, full).
+ * Replaces the overlap and projection products of EigenSolver::orthogonalize_gpu /
+ * project_and_diag_gpu (src/solvers/EigenSolver.cu:195-233; scale = dV there). */
+LYNX_API int lynx_gram_mixed(lynx_ctx* ctx, const float* Y, const float* HY, long long ld, long long rows, int n,
+                             double scale, double* Ms, double* Hs);
+
+/* Subspace rotation of the mixed-precision pass: psi = Y W (device pointers; Y FP32 rows x n,
+ * column stride ld; W FP64 n x n column-major; psi FP64 rows x n, column stride ldp), on the
+ * tensor cores with exact int8 slices.  Ms is the overlap of Y (Ms_ii = scale |y_i|^2, any
+ * positive scale): its diagonal sets the per-state power-of-two scaling.  n <= 1551.
+ * Replaces EigenSolver::rotate_orbitals_gpu (src/solvers/EigenSolver.cu:312-329). */
+LYNX_API int lynx_rotate_mixed(lynx_ctx* ctx, const float* Y, long long ld, long long rows, const double* Ms,
+                               const double* W, int n, double* psi, long long ldp);
+
+/* Diagnostic, no counterpart in the reference: one CTA waits, with at most `spins` tries
+ * (1 .. 2^20), for an mbarrier phase that nothing completes, with the same bounded wait the
+ * pipelined kernels use for their copies.  The wait gives up and the kernel returns; the call
+ * returns LYNX_ERR_TIMEOUT and the context stays usable.  Exercises the timeout error path
+ * without a hang. */
+LYNX_API int lynx_selftest_wait_timeout(lynx_ctx* ctx, int spins);
 
 /* hpsi += Vnl psi, as lynx_nonlocal_apply, but with no device allocation: the projector
  * coefficients live in a fixed 8 MiB device array inside the library (total projectors x ncol
@@ -247,7 +275,9 @@ LYNX_API int lynx_time_filter_step(lynx_ctx* ctx, const double* veff, int ncol, 
  * reference: its GPU path sizes d_alpha once for Nband columns in Hamiltonian::setup_gpu
  * (src/operators/Hamiltonian.cu:473) and has no per-call variant.  The array is shared by all
  * contexts on a device, so calls overlapping in time race; the first call on a device does
- * one-time set-up and should come before any stream capture.  Real (Gamma-point) FP64 only. */
+ * one-time set-up and should come before any stream capture.  The array's device address is
+ * resolved once per device and kept: it does not survive cudaDeviceReset.  Real (Gamma-point)
+ * FP64 only. */
 LYNX_API int lynx_nonlocal_apply_noalloc(lynx_ctx* ctx, const double* psi, double* hpsi, int ncol, int ld);
 
 /* Execution options of a context (no counterpart in the reference; both settings compute the

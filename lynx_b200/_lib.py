@@ -82,6 +82,10 @@ _SIGNATURES = {
     "lynx_occupations": (_c_int, [_pd, _c_int, _c_double, _c_double, _c_int, _pd]),
     "lynx_time_filter_step": (_c_int, [_p, _p, _c_int, _c_int, _c_int, _c_int, _pd]),
     "lynx_launch_count": (ctypes.c_longlong, [_c_int]),
+    "lynx_gram_mixed": (_c_int, [_p, _p, _p, ctypes.c_longlong, ctypes.c_longlong, _c_int, _c_double, _p, _p]),
+    "lynx_rotate_mixed": (_c_int, [_p, _p, ctypes.c_longlong, ctypes.c_longlong, _p, _p, _c_int, _p,
+                                   ctypes.c_longlong]),
+    "lynx_selftest_wait_timeout": (_c_int, [_p, _c_int]),
 }
 
 EXPORTED = tuple(_SIGNATURES)

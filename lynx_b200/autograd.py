@@ -4,13 +4,16 @@
   point).  H is symmetric on the grid (symmetric FD stencil, diagonal Veff, Vnl = dV chi Gamma
   chi^T), so the adjoint with respect to the orbitals is H itself, grad_psi = H grad_y, and with
   respect to the potential grad_Veff = sum_n grad_y_n * psi_n.
-* ``nonlocal_energy(ctx, psi, positions, occ, occfac)``: E_nl = occfac sum_n f_n sum_p Gamma_p
-  alpha_{p,n}^2 (alpha = dV chi^T psi_n); grad_psi_n = 2 occfac f_n dV (Vnl psi_n) (d alpha / d psi
-  = dV chi, and Vnl psi = chi Gamma alpha), and grad_positions = -F with F the nonlocal forces of
-  lynx_nonlocal_force (the formula of the reference's Forces::compute_nonlocal,
-  src/physics/Forces.cpp:509-797).  The projector tables of the context must belong to
-  ``positions``; the position gradient is along the lattice directions (Cartesian for orthogonal
-  cells).
+* ``nonlocal_energy(ctx, psi, positions, occ, occfac, psp)``: E_nl = occfac sum_n f_n sum_p
+  Gamma_p alpha_{p,n}^2 (alpha = dV chi^T psi_n); grad_psi_n = 2 occfac f_n dV (Vnl psi_n)
+  (d alpha / d psi = dV chi, and Vnl psi = chi Gamma alpha), and grad_positions = -F with F the
+  nonlocal forces of lynx_nonlocal_force (the formula of the reference's
+  Forces::compute_nonlocal, src/physics/Forces.cpp:509-797).  With a pseudopotential ``psp``
+  the forward pass rebuilds the context's projector tables at ``positions`` (what the
+  reference's NonlocalProjector::setup does for new atom positions), so the energy is a
+  function of the positions; without one, the context's current tables are used and must
+  belong to ``positions``.  The position gradient is along the lattice directions (Cartesian
+  for orthogonal cells).
 
 Orbitals are torch CUDA tensors of shape (ncol, Nd), float64 (the layout lynx_b200.solver takes
 without copies); the computation runs in liblynxb200.so.
@@ -46,7 +49,11 @@ def _make_fns():
 
     class NonlocalEnergy(torch.autograd.Function):
         @staticmethod
-        def forward(fctx, psi, positions, ctx, occ, occfac):
+        def forward(fctx, psi, positions, ctx, occ, occfac, psp):
+            if psp is not None:
+                from . import pseudo
+                R = positions.detach().cpu().numpy().astype(np.float64)
+                ctx.set_nonlocal(pseudo.nonlocal_tables(ctx.cell, R, psp))
             occ = np.asarray(occ, dtype=np.float64)
             f, e = solver.NonlocalProjector(ctx).force(psi.contiguous(), occ, occfac=occfac)
             fctx.ctx = ctx
@@ -67,7 +74,7 @@ def _make_fns():
                 grad_psi = grad_e * w * vnl
             if fctx.needs_input_grad[1]:
                 grad_pos = -grad_e.to(device=fctx.force.device, dtype=fctx.force.dtype) * fctx.force
-            return grad_psi, grad_pos, None, None, None
+            return grad_psi, grad_pos, None, None, None, None
 
     return HamiltonianApply, NonlocalEnergy
 
@@ -87,6 +94,7 @@ def hamiltonian_apply(ctx, psi, veff):
     return _fns()[0].apply(psi, veff, ctx)
 
 
-def nonlocal_energy(ctx, psi, positions, occ, occfac: float = 2.0):
-    """E_nl of the orbitals psi, differentiable in psi and in the atom positions."""
-    return _fns()[1].apply(psi, positions, ctx, occ, occfac)
+def nonlocal_energy(ctx, psi, positions, occ, occfac: float = 2.0, psp=None):
+    """E_nl of the orbitals psi, differentiable in psi and in the atom positions (with ``psp``,
+    a lynx_b200.pseudo.Psp8, the projector tables are rebuilt at ``positions`` first)."""
+    return _fns()[1].apply(psi, positions, ctx, occ, occfac, psp)

@@ -293,6 +293,7 @@ struct SliceArgs {
     const float* y[2];
     long long ldy, rows, ldk, chunk;
     int npad;
+    int* nonfinite;   // set to 1 when an input element is NaN or Inf (may be null)
 };
 
 // One K chunk of one column of an FP32 block (blockIdx.z: Y or HY) -> exponent e and three int8
@@ -306,10 +307,13 @@ __global__ void __launch_bounds__(256) slice_i8_kernel(const SliceArgs a) {
     const long long rend = min(r1, a.rows);
     const float* col = a.y[op] + (long long)j * a.ldy;
     float m = 0.0f;
+    bool bad = false;  // fmaxf drops NaN, and slicing would turn it into zeros: flag it instead
     for (long long r = r0 + 4 * threadIdx.x; r < rend; r += 4 * blockDim.x) {
         const float4 v = *reinterpret_cast<const float4*>(col + r);
         m = fmaxf(fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y))), fmaxf(fabsf(v.z), fabsf(v.w)));
+        bad |= !(isfinite(v.x) && isfinite(v.y) && isfinite(v.z) && isfinite(v.w));
     }
+    if (bad && a.nonfinite) *a.nonfinite = 1;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
@@ -689,7 +693,7 @@ __global__ void __launch_bounds__(128)
 
 int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows, int n, double dV,
                    const GramPlan& p, void* work, size_t work_bytes, double* Ms, double* Hs, int* err,
-                   cudaStream_t st) {
+                   int* nonfinite, cudaStream_t st) {
     if (work_bytes < p.work_bytes || (reinterpret_cast<uintptr_t>(work) & 255)) {
         set_error("Gram workspace too small or misaligned");
         return LYNX_ERR_BAD_ARG;
@@ -717,6 +721,7 @@ int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows
         sa.ldk = p.ldk;
         sa.chunk = chunk;
         sa.npad = p.npad;
+        sa.nonfinite = nonfinite;
         dim3 grid(p.nsplit, n, 2);
         slice_i8_kernel<<<grid, 256, 0, st>>>(sa);
         count_launch();

@@ -70,6 +70,7 @@ int pipe_shape_count(int R);
 // Rayleigh-Ritz Gram products Ms = dV Y^T Y (upper triangle), Hs = dV Y^T HY of FP32 blocks
 // (rows x n, column stride ld) on the tensor cores: exact int8-slice products, FP64 result,
 // Ms/Hs n x n column-major.  work: gram_plan(rows, n).work_bytes, 256-byte aligned.
+// nonfinite (device int, may be null) is set to 1 when Y or HY holds a NaN or Inf.
 struct GramPlan {
     long long ldk;      // padded K (rows) of the slice arrays
     int npad;           // N rounded up to the 128-state tile
@@ -79,7 +80,7 @@ struct GramPlan {
 GramPlan gram_plan(long long rows, int n);
 int launch_gram_i8(const float* Y, const float* HY, long long ld, long long rows, int n, double dV,
                    const GramPlan& p, void* work, size_t work_bytes, double* Ms, double* Hs, int* err,
-                   cudaStream_t st);
+                   int* nonfinite, cudaStream_t st);
 
 // Subspace rotation psi = Y W on the tensor cores (exact int8 slices, FP64 output written into
 // an unpadded layout with column stride ldp); gram_tc.cu.  launch_colexp must run on the

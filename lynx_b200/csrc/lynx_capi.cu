@@ -32,6 +32,7 @@
 #include "kernels.h"
 #include "lynx_common.cuh"
 #include "stencil.cuh"
+#include "stencil_pipe.cuh"
 
 namespace lynxb {
 
@@ -150,6 +151,31 @@ __global__ void hermitize_kernel(double2* A, int N) {
     }
 }
 
+// Sets *flag when an entry of the N x N column-major matrix A is NaN or Inf (comps doubles per
+// entry: 1 real, 2 complex; upper: only entries on or above the diagonal are valid).
+__global__ void nonfinite_kernel(const double* __restrict__ A, int N, int comps, int upper, int* __restrict__ flag) {
+    const long long n2 = (long long)N * N;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n2; t += (long long)gridDim.x * blockDim.x) {
+        const long long j = t / N, i = t - j * N;
+        if (upper && i > j) continue;
+        for (int q = 0; q < comps; ++q)
+            if (!isfinite(A[t * comps + q])) *flag = 1;
+    }
+}
+
+// One CTA waits, with at most `spins` tries, for a phase of an mbarrier that nothing completes:
+// the bounded wait of the pipelined kernels, made to run out.  It gives up, flags the error and
+// returns, which leaves the context usable.
+__global__ void wait_selftest_kernel(int spins, int* __restrict__ err) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && !mbar_wait(&bar, 0u, spins)) atomicExch(err, 1);
+}
+
 }  // namespace lynxb
 
 using namespace lynxb;
@@ -217,6 +243,11 @@ struct lynx_ctx {
     std::vector<int> h_img_ndc, h_img_atom, h_atom_nproj;
     std::vector<double> h_chi;
     DevBuf sbuf[4];  // stress: third gradient block, chi weighted by x, y, z relative positions
+    // lynx_time_filter_step with with_nonlocal = 2: events around the stencil kernel alone
+    bool time_stencil = false;
+    cudaEvent_t kt[2] = {nullptr, nullptr};
+    double kt_ms = 0.0;
+    int kt_n = 0;
 };
 
 namespace {
@@ -620,6 +651,18 @@ int pipe_launch_tuned(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* 
     return LYNX_OK;
 }
 
+// Adds the duration of the stencil launch bracketed by c->kt[0] (recorded before it) and an event
+// recorded now; waits for it.
+int stencil_time_add(lynx_ctx* c) {
+    LYNX_CUDA_TRY(cudaEventRecord(c->kt[1], c->stream));
+    LYNX_CUDA_TRY(cudaEventSynchronize(c->kt[1]));
+    float ms = 0.0f;
+    LYNX_CUDA_TRY(cudaEventElapsedTime(&ms, c->kt[0], c->kt[1]));
+    c->kt_ms += ms;
+    c->kt_n += 1;
+    return LYNX_OK;
+}
+
 // One Chebyshev step out = a H x + b x + d xold (H with the nonlocal term when tables are set).
 // With the fused nonlocal path, xs_in (optional) is the compact sphere-point copy of x written
 // by the previous step, and xs_out (optional) receives the compact copy of out; *xs_written
@@ -670,13 +713,17 @@ int cheb_step(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* xold, lo
                 LYNX_TRY(launch_nl_expand<T>(*nl, c->nlW.as<T>(), ldw, ncol, c->alpha.as<T>(), ncolp, c->stream));
                 PipeNLHost nh{c->nlW.p, ldw, nm->ptmap.as<int>(), nm->mp, nm->rowstart.as<int>(), &nm->rowstart_h,
                               xs_out};
+                if (c->time_stencil) LYNX_CUDA_TRY(cudaEventRecord(c->kt[0], c->stream));
                 LYNX_TRY(pipe_launch_tuned<T, S>(c, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
                                                  &nh));
+                if (c->time_stencil) LYNX_TRY(stencil_time_add(c));
                 if (xs_written) *xs_written = (xs_out != nullptr);
                 return LYNX_OK;
             }
         }
+        if (c->time_stencil) LYNX_CUDA_TRY(cudaEventRecord(c->kt[0], c->stream));
         LYNX_TRY(pipe_launch_tuned<T, S>(c, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, nullptr));
+        if (c->time_stencil) LYNX_TRY(stencil_time_add(c));
     } else {
         LYNX_TRY(launch_cheb_step<T, S>(geom(c), x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr, c->stream));
     }
@@ -846,11 +893,25 @@ namespace {
         }                                                                 \
     } while (0)
 
+// Flags (device int) a NaN or Inf among the entries of the N x N matrix A (asynchronous).
+int check_finite(lynx_ctx* c, const double* A, int N, int comps, bool upper, int* flag) {
+    const long long n2 = (long long)N * N;
+    const int blocks = (int)std::min<long long>((n2 + 255) / 256, 148LL * 8);
+    nonfinite_kernel<<<blocks, 256, 0, c->stream>>>(A, N, comps, upper ? 1 : 0, flag);
+    count_launch();
+    LYNX_CUDA_TRY(cudaGetLastError());
+    return LYNX_OK;
+}
+
 int finish_rr(lynx_ctx* c, int N, double* eig_host) {
-    int info[2] = {0, 0};
-    LYNX_CUDA_TRY(cudaMemcpyAsync(info, c->info.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    int info[3] = {0, 0, 0};
+    LYNX_CUDA_TRY(cudaMemcpyAsync(info, c->info.p, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     LYNX_CUDA_TRY(cudaMemcpyAsync(eig_host, c->eigd.p, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (info[2] != 0) {
+        set_error("non-finite entries in the overlap or projected Hamiltonian (NaN/Inf in the orbitals or Veff)");
+        return LYNX_ERR_NONFINITE;
+    }
     if (info[0] != 0) {
         set_error("Cholesky factorization of the overlap failed (info=%d)", info[0]);
         return info[0] > 0 ? LYNX_ERR_CHOL_FAIL : LYNX_ERR_BAD_ARG;
@@ -885,8 +946,9 @@ int rr_small_real(lynx_ctx* c, int N) {
                                              N, c->eigd.as<double>(), &lw2));
     const int lw = std::max(lw1, lw2);
     LYNX_TRY(c->solver_work.ensure((size_t)lw * sizeof(double)));
-    int* info = c->info.as<int>();
-    LYNX_CUDA_TRY(cudaMemsetAsync(info, 0, 2 * sizeof(int), c->stream));
+    int* info = c->info.as<int>();  // zeroed by rr_alloc_small
+    LYNX_TRY(check_finite(c, Ms, N, 1, true, info + 2));
+    LYNX_TRY(check_finite(c, Hs, N, 1, false, info + 2));
     CUSOLVER_TRY(cusolverDnDpotrf(c->cusolver, CUBLAS_FILL_MODE_UPPER, N, Ms, N, c->solver_work.as<double>(), lw,
                                   info));
     CUBLAS_TRY(cublasDtrsm(c->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
@@ -915,9 +977,11 @@ int rr_alloc_small(lynx_ctx* c, int N, size_t elem) {
     LYNX_TRY(c->Ms.ensure(nn * elem));
     LYNX_TRY(c->Hs.ensure(nn * elem));
     LYNX_TRY(c->eigd.ensure(N * sizeof(double)));
-    LYNX_TRY(c->info.ensure(2 * sizeof(int)));
+    LYNX_TRY(c->info.ensure(3 * sizeof(int)));
     CUBLAS_TRY(cublasSetStream(c->cublas, c->stream));
     CUSOLVER_TRY(cusolverDnSetStream(c->cusolver, c->stream));
+    // info[0]: potrf, info[1]: syevd, info[2]: a NaN / Inf seen in the products or their inputs
+    LYNX_CUDA_TRY(cudaMemsetAsync(c->info.p, 0, 3 * sizeof(int), c->stream));
     return LYNX_OK;
 }
 
@@ -943,7 +1007,7 @@ int rayleigh_ritz_mixed_real(lynx_ctx* c, const float* Y32, const float* HY32, l
     LYNX_TRY(c->gwork.ensure(plan.work_bytes));
     if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
     LYNX_TRY(launch_gram_i8(Y32, HY32, ldb, ldb, N, c->dV, plan, c->gwork.p, c->gwork.bytes, c->Ms.as<double>(),
-                            c->Hs.as<double>(), c->errflag.as<int>(), c->stream));
+                            c->Hs.as<double>(), c->errflag.as<int>(), c->info.as<int>() + 2, c->stream));
     if (rot_supported(N)) {
         // rotation on the tensor cores, straight from the FP32 block into the caller's psi
         const RotPlan rp = rot_plan(ldb, N);
@@ -966,7 +1030,7 @@ int rayleigh_ritz_cplx(lynx_ctx* c, const double2* Y, long long ldY, const doubl
     LYNX_TRY(c->Ms.ensure(nn * sizeof(double2)));
     LYNX_TRY(c->Hs.ensure(nn * sizeof(double2)));
     LYNX_TRY(c->eigd.ensure(N * sizeof(double)));
-    LYNX_TRY(c->info.ensure(2 * sizeof(int)));
+    LYNX_TRY(c->info.ensure(3 * sizeof(int)));
     cuDoubleComplex* Ms = c->Ms.as<cuDoubleComplex>();
     cuDoubleComplex* Hs = c->Hs.as<cuDoubleComplex>();
     const cuDoubleComplex* Yz = reinterpret_cast<const cuDoubleComplex*>(Y);
@@ -991,7 +1055,9 @@ int rayleigh_ritz_cplx(lynx_ctx* c, const double2* Y, long long ldY, const doubl
     LYNX_TRY(c->solver_work.ensure((size_t)lw * sizeof(cuDoubleComplex)));
     int* info = c->info.as<int>();
     cuDoubleComplex* work = c->solver_work.as<cuDoubleComplex>();
-    LYNX_CUDA_TRY(cudaMemsetAsync(info, 0, 2 * sizeof(int), c->stream));
+    LYNX_CUDA_TRY(cudaMemsetAsync(info, 0, 3 * sizeof(int), c->stream));
+    LYNX_TRY(check_finite(c, reinterpret_cast<const double*>(Ms), N, 2, true, info + 2));
+    LYNX_TRY(check_finite(c, reinterpret_cast<const double*>(Hs), N, 2, false, info + 2));
     CUSOLVER_TRY(cusolverDnZpotrf(c->cusolver, CUBLAS_FILL_MODE_UPPER, N, Ms, N, work, lw, info));
     CUBLAS_TRY(cublasZtrsm(c->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, CUBLAS_DIAG_NON_UNIT,
                            N, N, &one, Ms, N, Hs, N));
@@ -1370,6 +1436,8 @@ int lynx_destroy(lynx_ctx* c) {
     c->fones.release();
     for (auto& b : c->sbuf) b.release();
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    for (cudaEvent_t e : c->kt)
+        if (e) cudaEventDestroy(e);
     for (auto& b : c->nl_layout_bufs) b.release();
     for (auto& kv : c->nl_maps) {
         kv.second.ptmap.release();
@@ -1679,9 +1747,11 @@ int lynx_hamiltonian_apply_kpt(lynx_ctx* c, const double* psi, const double* vef
 
 int lynx_nonlocal_apply(lynx_ctx* c, const double* psi, double* hpsi, int ncol, int ld) {
     LYNX_CHECK_ARG(c && psi && hpsi, "null pointer");
+    LYNX_CHECK_ARG(ncol > 0, "ncol must be positive");
+    const long long l = ld > 0 ? ld : c->Nd;
+    LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
     if (!c->has_nl) return LYNX_OK;
     LYNX_TRY(activate(c));
-    const long long l = ld > 0 ? ld : c->Nd;
     const int ncolp = ((ncol + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
     LYNX_TRY(c->alpha.ensure(sizeof(double) * (size_t)c->nl.total_proj * ncolp));
     LYNX_TRY(launch_nl_gather<double>(c->nl, psi, l, ncol, c->alpha.as<double>(), ncolp, c->dV, c->stream));
@@ -1690,9 +1760,11 @@ int lynx_nonlocal_apply(lynx_ctx* c, const double* psi, double* hpsi, int ncol, 
 
 int lynx_nonlocal_apply_kpt(lynx_ctx* c, const double* psi, double* hpsi, int ncol, int ld) {
     LYNX_CHECK_ARG(c && psi && hpsi, "null pointer");
+    LYNX_CHECK_ARG(ncol > 0, "ncol must be positive");
+    const long long l = ld > 0 ? ld : c->Nd;
+    LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
     if (!c->has_nl) return LYNX_OK;
     LYNX_TRY(activate(c));
-    const long long l = ld > 0 ? ld : c->Nd;
     const int ncolp = ((ncol + kNLColBlock - 1) / kNLColBlock) * kNLColBlock;
     LYNX_TRY(c->alpha.ensure(sizeof(double2) * (size_t)c->nl.total_proj * ncolp));
     LYNX_TRY(launch_nl_gather<double2>(c->nl, reinterpret_cast<const double2*>(psi), l, ncol,
@@ -1835,12 +1907,19 @@ int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precisi
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     int st = LYNX_OK;
+    if (with_nonlocal == 2) {  // time the stencil kernel alone (its nonlocal term fused when it applies)
+        for (int i = 0; i < 2; ++i)
+            if (!c->kt[i]) LYNX_CUDA_TRY(cudaEventCreate(&c->kt[i]));
+        c->kt_ms = 0.0;
+        c->kt_n = 0;
+    }
     const float* v32 = nullptr;
     const double* v64 = nullptr;
     if (precision == LYNX_PREC_MIXED) st = veff_layout<float>(c, veff, nxp, &v32);
     else st = veff_layout<double>(c, veff, nxp, &v64);
     for (int r = -1; r < reps && st == LYNX_OK; ++r) {  // r = -1: untimed warm-up launch
         if (r == 0) cudaEventRecord(e0, c->stream);
+        c->time_stencil = (with_nonlocal == 2 && r >= 0);
         const int a = (r + 3) % 3, b = (r + 4) % 3, o = (r + 5) % 3;
         if (precision == LYNX_PREC_FP64)
             st = cheb_step<double>(c, nxp, c->wbuf[a].as<double>(), ldb, c->wbuf[b].as<double>(), ldb,
@@ -1849,6 +1928,7 @@ int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precisi
             st = cheb_step<float>(c, nxp, c->wbuf[a].as<float>(), ldb, c->wbuf[b].as<float>(), ldb,
                                   c->wbuf[o].as<float>(), ldb, v32, ncol, 0.5, -0.1, -0.25, false);
     }
+    c->time_stencil = false;
     cudaEventRecord(e1, c->stream);
     cudaEventSynchronize(e1);
     float ms = 0;
@@ -1859,7 +1939,7 @@ int lynx_time_filter_step(lynx_ctx* c, const double* veff, int ncol, int precisi
     if (st != LYNX_OK) return st;
     LYNX_CUDA_TRY(cudaGetLastError());
     LYNX_TRY(check_errflag(c));
-    *ms_per_step = ms / reps;
+    *ms_per_step = (with_nonlocal == 2) ? (c->kt_n ? c->kt_ms / c->kt_n : 0.0) : ms / reps;
     return LYNX_OK;
 }
 
@@ -1921,8 +2001,11 @@ int lynx_occupations(const double* eigs, int n, double ef, double beta, int smea
 // The scratch array is shared by every context on a device: calls that overlap in time (two
 // streams or two host threads on one device) race on it and must be serialised by the caller.
 // The first call on a device resolves the array's address (cudaGetSymbolAddress, which also
-// loads the module) and should be made once before any stream capture is begun.  Nothing in
-// the scratch needs to start at zero: the gather writes every alpha element the scatter reads.
+// loads the module) and should be made once before any stream capture is begun.  The address is
+// kept for the life of the process: after cudaDeviceReset (which frees every allocation and
+// context of the process, so no lynx context survives it either) the library must be reloaded
+// before this entry point is used again.  Nothing in the scratch needs to start at zero: the
+// gather writes every alpha element the scatter reads.
 // ---------------------------------------------------------------------------------------------
 namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(8) << 20;  // 8 MiB = 1 Mi doubles
@@ -2222,6 +2305,58 @@ extern "C" int lynx_set_option(lynx_ctx* c, int option, int value) {
         case LYNX_OPT_FUSE_NONLOCAL: c->fuse_nl = value != 0; return LYNX_OK;
         default: set_error("unknown option %d", option); return LYNX_ERR_BAD_ARG;
     }
+}
+
+extern "C" int lynx_gram_mixed(lynx_ctx* c, const float* Y, const float* HY, long long ld, long long rows, int n,
+                               double scale, double* Ms, double* Hs) {
+    LYNX_CHECK_ARG(c && Y && HY && Ms && Hs, "null pointer");
+    LYNX_CHECK_ARG(n > 0 && rows > 0 && ld >= rows, "need n > 0, rows > 0 and ld >= rows");
+    LYNX_TRY(activate(c));
+    const GramPlan plan = gram_plan(rows, n);
+    LYNX_TRY(c->gwork.ensure(plan.work_bytes));
+    LYNX_TRY(c->info.ensure(3 * sizeof(int)));
+    if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
+    int* bad = c->info.as<int>() + 2;
+    LYNX_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
+    LYNX_TRY(launch_gram_i8(Y, HY, ld, rows, n, scale, plan, c->gwork.p, c->gwork.bytes, Ms, Hs, c->errflag.as<int>(),
+                            bad, c->stream));
+    int h = 0;
+    LYNX_CUDA_TRY(cudaMemcpyAsync(&h, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    LYNX_TRY(check_errflag(c));  // synchronises the stream
+    if (h) {
+        set_error("NaN or Inf in the FP32 blocks of the Gram products");
+        return LYNX_ERR_NONFINITE;
+    }
+    return LYNX_OK;
+}
+
+extern "C" int lynx_rotate_mixed(lynx_ctx* c, const float* Y, long long ld, long long rows, const double* Ms,
+                                 const double* W, int n, double* psi, long long ldp) {
+    LYNX_CHECK_ARG(c && Y && Ms && W && psi, "null pointer");
+    LYNX_CHECK_ARG(n > 0 && rows > 0 && ld >= rows && ldp >= rows, "need n > 0, rows > 0, ld >= rows, ldp >= rows");
+    if (!rot_supported(n)) {
+        set_error("the tensor-core rotation takes at most %d states", (int)(200 * 1024 / (33 * sizeof(float))));
+        return LYNX_ERR_UNSUPPORTED;
+    }
+    LYNX_TRY(activate(c));
+    const RotPlan rp = rot_plan(rows, n);
+    LYNX_TRY(c->rwork.ensure(rp.work_bytes));
+    if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
+    LYNX_TRY(launch_colexp(Ms, n, c->rwork.p, rp, rows, c->stream));
+    LYNX_TRY(launch_rot_i8(Y, ld, rows, 1, 1, W, n, rp, c->rwork.p, c->rwork.bytes, psi, ldp, c->errflag.as<int>(),
+                           c->stream));
+    return check_errflag(c);
+}
+
+extern "C" int lynx_selftest_wait_timeout(lynx_ctx* c, int spins) {
+    LYNX_CHECK_ARG(c != nullptr, "null context");
+    LYNX_CHECK_ARG(spins >= 1 && spins <= (1 << 20), "spins must lie in [1, 2^20]");
+    LYNX_TRY(activate(c));
+    if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
+    wait_selftest_kernel<<<1, 32, 0, c->stream>>>(spins, c->errflag.as<int>());
+    count_launch();
+    LYNX_CUDA_TRY(cudaGetLastError());
+    return check_errflag(c);
 }
 
 extern "C" int lynx_nonlocal_apply_noalloc(lynx_ctx* c, const double* psi, double* hpsi, int ncol, int ld) {

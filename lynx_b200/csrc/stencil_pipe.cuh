@@ -107,10 +107,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
-// Bounded wait for the phase with the given parity; returns false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the phase with the given parity (at most `limit` tries); returns false on
+// timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit = kSpinLimit) {
     const uint32_t addr = smem_u32(bar);
-    for (int i = 0; i < kSpinLimit; ++i) {
+    for (int i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

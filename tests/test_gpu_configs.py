@@ -1,0 +1,147 @@
+"""Parity at the benchmark configurations, against the reference CPU hot path (oracle/_ref: the
+reference's EigenSolver / Hamiltonian / NonlocalProjector sources compiled unmodified), on the
+same seeded inputs and the same synthetic Si-like pseudopotential.
+
+  * C1, Si8 on a 30^3 grid, 24 states: two FP64 CheFSI passes (degree 20) with the reference's
+    cutoff policy between them (src/solvers/EigenSolver.cpp:817, src/scf/SCF.cpp:421-431):
+    Ritz values within 1e-9 Ha, Ritz subspaces within 1e-7;
+  * C2, Si64 on a 60^3 grid, 160 states: one FP64 pass, Ritz values within 1e-9 Ha;
+  * C3, Si216 (atoms displaced by N(0, 0.02 Bohr)) on the 90^3 grid: the degree-20 filter on a
+    sample of 4 of the 520 columns (the filter acts on every column independently), FP64 within
+    1e-10 and FP32 within 2e-5 per column of the reference's FP64 filter;
+  * C3 on a 45^3 grid with all 520 states (so that the reference's pass runs in seconds): one
+    FP64 pass, Ritz values within 1e-9 Ha and subspace within 1e-7 -- the Rayleigh-Ritz at the
+    full state count, five 128-state tiles with a ragged last one;
+  * C5 geometry (Si64, 60^3, 160 states, atoms displaced by N(0, 0.05 Bohr), diagonal strain
+    uniform(+-1%)) converged: FP64 and mixed passes iterated from the same start at fixed V_eff
+    until the FP64 occupied Ritz values stop moving; the occupied Ritz values then agree within
+    1e-6 Ha and the nonlocal forces computed from the two sets of orbitals (Fermi-Dirac
+    occupations, 0.001 Ha smearing) within 1e-4 Ha/Bohr.
+V_eff is the seeded synthetic potential (Gaussian wells on the atoms plus N(0, 1e-3 Ha) noise):
+no converged Si potential is available."""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import rel_err, subspace_distance
+from lynx_b200 import cell as C
+from lynx_b200 import pseudo as P
+from oracle import ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(reps, grid, displace, seed, psp_path, strain=None):
+    from lynx_b200 import solver
+    cl, pos = C.diamond_si(reps, grid, displace=displace, strain=strain, seed=seed)
+    V = C.synthetic_veff_separable(cl, pos, noise=1e-3, seed=seed)
+    tab = P.nonlocal_tables(cl, pos, P.read_psp8(psp_path))
+    ctx = solver.Context(cl)
+    ctx.set_nonlocal(tab)
+    R = ref.RefLynx(cl, pos, psp_path, threads=os.cpu_count())
+    return cl, pos, V, ctx, R
+
+
+def test_c1_si8_two_fp64_passes(synth_psp8):
+    from lynx_b200 import solver
+    cl, pos, V, ctx, R = _system(1, 30, 0.0, 11, synth_psp8)
+    lo, hi = R.lanczos(V)
+    lc = 0.5 * (lo + hi)
+    psi0 = C.random_orbitals(ctx.nd, 24, seed=101)
+    es = solver.EigenSolver(ctx, "fp64")
+    psi_r, psi = psi0.copy(order="F"), psi0.copy(order="F")
+    lc_r, lc_g, emin_r, emin_g = lc, lc, lo, lo
+    for _ in range(2):
+        psi_r, eig_r = R.solve(psi_r, V, lc_r, emin_r, hi, 20)
+        psi, eig = es.solve(psi, V, lc_g, emin_g, hi, 20)
+        assert np.abs(eig - eig_r).max() < 1e-9
+        assert subspace_distance(psi, psi_r) < 1e-7
+        lc_r, emin_r = eig_r[-1] + 0.1, eig_r[0]
+        lc_g, emin_g = es.lambda_cutoff(), eig[0]
+        assert abs(lc_g - lc_r) < 1e-9
+    ctx.close()
+
+
+def test_c2_si64_fp64_pass(synth_psp8):
+    from lynx_b200 import solver
+    cl, pos, V, ctx, R = _system(2, 60, 0.0, 12, synth_psp8)
+    lo, hi = R.lanczos(V)
+    lc = 0.5 * (lo + hi)
+    psi0 = C.random_orbitals(ctx.nd, 160, seed=102)
+    _, eig_r = R.solve(psi0, V, lc, lo, hi, 20)
+    _, eig = solver.EigenSolver(ctx, "fp64").solve(psi0, V, lc, lo, hi, 20)
+    assert np.abs(eig - eig_r).max() < 1e-9
+    ctx.close()
+
+
+def test_c3_si216_filter_column_sample(synth_psp8):
+    from lynx_b200 import solver
+    cl, pos, V, ctx, R = _system(3, 90, 0.02, 2024, synth_psp8)
+    lo, hi = R.lanczos(V, maxit=200)
+    lc = 0.5 * (lo + hi)
+    X = C.random_orbitals(ctx.nd, 4, seed=103)
+    Y_ref = R.chebyshev_filter(X, V, lc, lo, hi, 20)
+    es = solver.EigenSolver(ctx)
+    Y64 = es.chebyshev_filter(X, V, lc, lo, hi, 20, precision="fp64")
+    assert rel_err(Y64, Y_ref) < 1e-10
+    Y32 = es.chebyshev_filter(X, V, lc, lo, hi, 20, precision="mixed")
+    for j in range(4):
+        assert rel_err(Y32[:, j], Y_ref[:, j]) < 2e-5
+    ctx.close()
+
+
+def test_c3_si216_coarse_grid_fp64_pass_520_states(synth_psp8):
+    from lynx_b200 import solver
+    cl, pos, V, ctx, R = _system(3, 45, 0.02, 2024, synth_psp8)
+    lo, hi = R.lanczos(V)
+    lc = 0.5 * (lo + hi)
+    psi0 = C.random_orbitals(ctx.nd, 520, seed=104)
+    psi_r, eig_r = R.solve(psi0, V, lc, lo, hi, 20)
+    psi, eig = solver.EigenSolver(ctx, "fp64").solve(psi0, V, lc, lo, hi, 20)
+    assert np.abs(eig - eig_r).max() < 1e-9
+    assert subspace_distance(psi[:, :432], psi_r[:, :432]) < 1e-7
+    ctx.close()
+
+
+def test_c5_converged_mixed_vs_fp64_eigenvalues_and_forces(synth_psp8):
+    """CheFSI at fixed V_eff from one start: both precisions converge to the same occupied Ritz
+    values (<= 1e-6 Ha) and nonlocal forces (<= 1e-4 Ha/Bohr)."""
+    import torch
+    from lynx_b200 import solver
+    strain = np.random.default_rng(13).uniform(-0.01, 0.01, size=3)
+    cl, pos, V, ctx, R = _system(2, 60, 0.05, 13, synth_psp8, strain=strain)
+    nocc, N = 128, 160
+    es0 = solver.EigenSolver(ctx)
+    lo, hi = es0.lanczos_bounds(V)
+    g = torch.Generator(device="cuda").manual_seed(105)
+    start = (torch.rand((N, ctx.nd), generator=g, device="cuda", dtype=torch.float64) - 0.5).contiguous()
+    Vd = torch.from_numpy(V).cuda()
+    out = {}
+    for prec in ("fp64", "mixed"):
+        es = solver.EigenSolver(ctx, prec)
+        psi = start.clone()
+        lc, emin = 0.5 * (lo + hi), lo
+        prev = None
+        for it in range(100):
+            _, eig = es.solve(psi, Vd, lc, emin, hi, 20)
+            eig = np.asarray(eig)
+            lc, emin = es.lambda_cutoff(), float(eig[0])
+            if prev is not None and np.abs(eig[:nocc] - prev[:nocc]).max() < 1e-10:
+                break
+            prev = eig
+        out[prec] = (psi, eig, it)
+    psi64, eig64, it64 = out["fp64"]
+    psim, eigm, _ = out["mixed"]
+    assert it64 < 99, "FP64 passes did not converge"
+    assert np.abs(eigm[:nocc] - eig64[:nocc]).max() <= 1e-6
+    nel = 4.0 * len(pos)
+    forces = []
+    for psi, eig in ((psi64, eig64), (psim, eigm)):
+        ef = solver.fermi_level(eig, 2.0 * np.ones(N), nel, 1000.0)  # spin factor 2 in the weights
+        occ = solver.occupations(eig, ef, 1000.0)
+        f, _ = solver.NonlocalProjector(ctx).force(psi, occ, occfac=2.0)
+        forces.append(np.asarray(f))
+    assert np.abs(forces[0]).max() > 1e-3  # the displaced atoms feel real forces
+    assert np.abs(forces[1] - forces[0]).max() <= 1e-4
+    ctx.close()

@@ -227,8 +227,8 @@ def test_free_particle_known_answer(n):
 
 @pytest.mark.parametrize("nstates", [150])
 def test_mixed_pass_tensor_core_gram(system, nstates):
-    """Mixed precision real pass (FP32 filter, BF16x3 tensor-core Gram products with FP64
-    split-K reduction, FP64 subspace algebra) against the FP64 pass from the same start:
+    """Mixed precision real pass (FP32 filter, exact int8-slice tensor-core Gram products with
+    FP64 split-K reduction, FP64 subspace algebra) against the FP64 pass from the same start:
     more than one 128-state output tile, a ragged last tile.  Ritz values agree to 2e-5 Ha
     (FP32 filter rounding dominates), the spectrum stays ordered and both passes span the
     same subspace."""
