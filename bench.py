@@ -355,6 +355,10 @@ def main():
 
     for _ in range(args.warmup):
         one_pass(args.precision)
+    # the other precision's first pass runs the stencil autotuner for its own types: keep it out of
+    # the timed passes
+    other = "fp64" if args.precision == "mixed" else "mixed"
+    one_pass(other)
     natom = len(pos)
     nocc = 2 * natom  # 4 valence electrons per Si, 2 per state
 
@@ -377,7 +381,6 @@ def main():
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 1e3 / k
 
-    other = "fp64" if args.precision == "mixed" else "mixed"
     t_other = timed(other, max(1, min(2, args.steps)))
 
     lib.lynx_launch_count(1)

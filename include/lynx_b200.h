@@ -280,16 +280,21 @@ LYNX_API int lynx_selftest_wait_timeout(lynx_ctx* ctx, int spins);
  * FP64 only. */
 LYNX_API int lynx_nonlocal_apply_noalloc(lynx_ctx* ctx, const double* psi, double* hpsi, int ncol, int ld);
 
-/* Execution options of a context (no counterpart in the reference; both settings compute the
- * same results, bitwise):
+/* Execution options of a context (no counterpart in the reference).  The first two compute the
+ * same results with either setting, bitwise:
  *   LYNX_OPT_AUTOTUNE:       1 (default) times the compiled stencil launch shapes on the first
  *                            launch for each grid and column count and keeps the fastest; 0 uses
  *                            the default shape.
  *   LYNX_OPT_FUSE_NONLOCAL:  1 (default) adds the nonlocal term inside the stencil kernel when
  *                            the projector spheres are disjoint (real data, periodic orthogonal
  *                            cell, FD order 12), from a compact per-point expansion; 0 always
- *                            uses the separate gather and scatter kernels. */
-enum { LYNX_OPT_AUTOTUNE = 1, LYNX_OPT_FUSE_NONLOCAL = 2 };
+ *                            uses the separate gather and scatter kernels.
+ *   LYNX_OPT_TC_RAYLEIGH_RITZ: 1 (default) runs the mixed-precision pass's Gram products and
+ *                            rotation on the tensor cores (exact int8 slices, as accurate as
+ *                            FP64 products of the FP32 blocks to about 1e-8); 0 runs them as FP64
+ *                            library products on FP64 copies of the FP32 blocks (slower).
+ */
+enum { LYNX_OPT_AUTOTUNE = 1, LYNX_OPT_FUSE_NONLOCAL = 2, LYNX_OPT_TC_RAYLEIGH_RITZ = 3 };
 LYNX_API int lynx_set_option(lynx_ctx* ctx, int option, int value);
 
 /* Number of kernel launches this library issued since the last reset (diagnostic counter). */

@@ -4,24 +4,28 @@
 // the overlap and projected-Hamiltonian products of the Rayleigh-Ritz step).
 //
 // Precision (integer split, "Ozaki" scheme): the K range is cut into split chunks; in each
-// chunk every state column j is scaled by a power of two 2^-e_j (|y| 2^-e < 1/2) and written
-// as three signed 7-bit slices,
-//     y = 2^e (s1 2^-7 + s2 2^-14 + s3 2^-21) + r,   s_a in [-64, 64],  |r| <= 2^(e-22),
-// each slice rounded to nearest (unbiased).  The slice products with a+b <= 4 are formed by
-// tcgen05.mma kind::i8 into three int32 accumulators in tensor memory (one per weight
-// 2^-14, 2^-21, 2^-28), which is exact: no rounding at all happens in the tensor cores.
-// The epilogue combines the three levels exactly in FP64 and applies 2^(e_i+e_j); the split
-// partials are summed in FP64.  The only approximation is the slice representation
-// (relative 2^-20 of the column's largest element, unbiased), far below the FP32 rounding
-// of Y itself once summed over K.  (FP32-accumulating bf16 products were measured on this
-// hardware to carry an accumulation bias that grows with K, ~1e-4 relative at 7e5 points.)
+// chunk every state column j is rounded to a 23-bit integer on its own power-of-two scale,
+//     T = rint(y 2^(22-e)),  e = the exponent of the column's largest |y| (so |T| <= 2^22),
+// and T is written as three balanced base-256 digits, T = d1 2^16 + d2 2^8 + d3 with
+// d2, d3 in [-128, 127] and |d1| <= 64: three signed int8 slices whose digits have zero mean.
+// The slice products with a+b <= 5 (8 of the 9) are formed by tcgen05.mma kind::i8 into four
+// int32 accumulators in tensor memory (weights 2^-12, 2^-20, 2^-28, 2^-36 relative to
+// 2^(e_i+e_j)), which is exact: no rounding happens in the tensor cores.  The epilogue
+// combines the four levels in FP64 and applies 2^(e_i+e_j); the split partials are summed in
+// FP64.  The approximations are the rounding of T (half a unit in 2^22 of the column's
+// largest element, unbiased) and the one dropped product d3 d3' 2^-44, both far below the
+// FP32 rounding of Y itself once summed over K (the result is as accurate as an FP64 product
+// of the FP32 data to about 1e-8 of sqrt(Ms_ii Ms_jj)).  An earlier form with three 7-bit
+// slices and six products was measured at 2e-7 (Hs) and 1.4e-5 (rotation, relative to the
+// column maximum); FP32-accumulating bf16 products carry an accumulation bias that grows with
+// K, ~1e-4 relative at 7e5 points.
 //
 // Kernel structure (one CTA = one 128 x 128 output tile x one K chunk, 4 warps):
 //   warp 0 lane 0  : TMA producer, 2-stage ring of the 6 slice tiles (A s1..s3, B s1..s3),
 //                    128 rows x 128 int8 each, in the 128-byte-swizzled K-major layout;
-//   warp 1 lane 0  : MMA issuer, 24 MMAs per stage (4 K32 sub-steps x 6 slice products),
+//   warp 1 lane 0  : MMA issuer, 32 MMAs per stage (4 K32 sub-steps x 8 slice products),
 //                    then tcgen05.commit to release the stage;
-//   all 4 warps    : epilogue, tcgen05.ld of the three 128 x 128 int32 accumulators (warp w
+//   all 4 warps    : epilogue, tcgen05.ld of the four 128 x 128 int32 accumulators (warp w
 //                    owns TMEM lanes 32w..32w+31) and a store of the FP64 partial tile.
 // Ms needs only its upper triangle (the Cholesky reads it), so only tiles tm <= tn run.
 // Every mbarrier wait is bounded; a timeout sets the error flag, and tensor memory is
@@ -44,11 +48,13 @@ constexpr int BM = 128, BN = 128, BK = 128, STAGES = 2;  // BK: int8 K elements 
 constexpr int NSLICE = 3;
 constexpr int TILE_BYTES = BM * BK;                      // 16 KB, one slice tile
 constexpr int STAGE_BYTES = 2 * NSLICE * TILE_BYTES;     // A and B slices: 96 KB
-constexpr int TMEM_COLS = 512;                           // 3 accumulators x 128 columns, power of two
+constexpr int TMEM_COLS = 512;                           // 4 accumulators x 128 columns
 // Rotation: the epilogue splits each TMEM lane quarter's 128 columns into kRotParts parts, one
 // warp each (kRotParts * 4 warps; BN / kRotParts a multiple of 16).
 constexpr int kRotParts = 4, kRotThreads = 128 * kRotParts;
-constexpr int kMaxChunkSteps = 1365;  // 3 * 64 * 64 * 128 * 1365 < 2^31: int32 accumulators cannot overflow
+// One K element adds at most 64*128 + 128*128 + 128*64 = 2^15 to an accumulator level (|d1| <= 64,
+// |d2|, |d3| <= 128), so a K chunk of 511 steps x 128 rows keeps every int32 level below 2^31.
+constexpr int kMaxChunkSteps = 511;
 // kind::i8 instruction descriptor: D = S32 (bits 4-5 = 2), A = B = signed 8-bit (bits 7-9,
 // 10-12 = 1), K-major A and B, N>>3 at bits 17-22, M>>4 at bits 24-28.
 constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
@@ -222,12 +228,14 @@ __global__ void __launch_bounds__(128, 1)
                 for (int kk = 0; kk < BK / 32; ++kk) {
                     const uint64_t off = (uint64_t)(kk * 32) >> 4;  // K32 sub-step = 32 bytes along the row
                     const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
-                    mma_i8(tmem + 0, a[0] + off, b[0] + off, acc);        // weight 2^-14
-                    mma_i8(tmem + 128, a[0] + off, b[1] + off, acc);      // weight 2^-21
+                    mma_i8(tmem + 0, a[0] + off, b[0] + off, acc);        // weight 2^-12
+                    mma_i8(tmem + 128, a[0] + off, b[1] + off, acc);      // weight 2^-20
                     mma_i8(tmem + 128, a[1] + off, b[0] + off, 1u);
                     mma_i8(tmem + 256, a[0] + off, b[2] + off, acc);      // weight 2^-28
                     mma_i8(tmem + 256, a[1] + off, b[1] + off, 1u);
                     mma_i8(tmem + 256, a[2] + off, b[0] + off, 1u);
+                    mma_i8(tmem + 384, a[1] + off, b[2] + off, acc);      // weight 2^-36
+                    mma_i8(tmem + 384, a[2] + off, b[1] + off, 1u);
                 }
                 mma_commit(&empty[s]);
             }
@@ -245,17 +253,17 @@ __global__ void __launch_bounds__(128, 1)
             const uint32_t lb = (uint32_t)(warp * 32) << 16;
 #pragma unroll 1
             for (int c0 = 0; c0 < BN; c0 += 16) {
-                uint32_t r2[16], r3[16], r4[16];
+                uint32_t r2[16], r3[16], r4[16], r5[16];
                 tmem_ld16(tmem + lb + (uint32_t)c0, r2);
                 tmem_ld16(tmem + lb + 128u + (uint32_t)c0, r3);
                 tmem_ld16(tmem + lb + 256u + (uint32_t)c0, r4);
+                tmem_ld16(tmem + lb + 384u + (uint32_t)c0, r5);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 double v[16];
 #pragma unroll
                 for (int t = 0; t < 16; ++t) {
-                    // exact: the three terms span bits 2^17 .. 2^-28 (< 53 bits)
-                    const double x = (double)(int)r2[t] * 0x1p-14 + (double)(int)r3[t] * 0x1p-21 +
-                                     (double)(int)r4[t] * 0x1p-28;
+                    const double x = (double)(int)r2[t] * 0x1p-12 + (double)(int)r3[t] * 0x1p-20 +
+                                     (double)(int)r4[t] * 0x1p-28 + (double)(int)r5[t] * 0x1p-36;
                     v[t] = x * sa * pow2d(eB[n0 + c0 + t]);  // exact: powers of two
                 }
                 double2* dst = reinterpret_cast<double2*>(wrow + c0);
@@ -275,16 +283,20 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
-// t = y 2^(7-e), |t| < 64 -> three int8 slices, each rounded to nearest (all steps exact).
+// T (|T| <= 2^22) -> balanced base-256 digits T = d1 2^16 + d2 2^8 + d3, d2, d3 in [-128, 127],
+// |d1| <= 64 (exact integer steps).
+__device__ __forceinline__ void digits3(int T, int8_t& a, int8_t& b, int8_t& c) {
+    const int d3 = ((T & 0xFF) ^ 0x80) - 0x80;
+    const int T1 = (T - d3) >> 8;
+    const int d2 = ((T1 & 0xFF) ^ 0x80) - 0x80;
+    a = (int8_t)((T1 - d2) >> 8);
+    b = (int8_t)d2;
+    c = (int8_t)d3;
+}
+// t = y 2^(22-e), |t| < 2^22 (an exact power-of-two scaling of FP32 y) -> three int8 slices of
+// rint(t).
 __device__ __forceinline__ void slice3(float t, int8_t& a, int8_t& b, int8_t& c) {
-    const float fa = rintf(t);
-    t = (t - fa) * 128.0f;
-    const float fb = rintf(t);
-    t = (t - fb) * 128.0f;
-    const float fc = rintf(t);
-    a = (int8_t)(int)fa;
-    b = (int8_t)(int)fb;
-    c = (int8_t)(int)fc;
+    digits3(__float2int_rn(t), a, b, c);
 }
 
 struct SliceArgs {
@@ -322,10 +334,10 @@ __global__ void __launch_bounds__(256) slice_i8_kernel(const SliceArgs a) {
 #pragma unroll
     for (int w = 1; w < 8; ++w) m = fmaxf(m, red[w]);
     int E = 0;
-    if (m > 0.0f) frexpf(m, &E);  // m = f 2^E, f in [1/2, 1)
-    const int e = (m > 0.0f) ? E + 1 : 0;  // |y| 2^-e < 1/2
+    if (m > 0.0f) frexpf(m, &E);  // m = f 2^E, f in [1/2, 1): |y| 2^(22-E) < 2^22
+    const int e = (m > 0.0f) ? E : 0;
     if (threadIdx.x == 0) a.e[op][(long long)split * a.npad + j] = e;
-    const float sc = pow2f(7 - e);
+    const float sc = pow2f(22 - e);
     int8_t* o1 = a.s[3 * op] + (long long)j * a.ldk;
     int8_t* o2 = a.s[3 * op + 1] + (long long)j * a.ldk;
     int8_t* o3 = a.s[3 * op + 2] + (long long)j * a.ldk;
@@ -446,12 +458,13 @@ namespace {
 // exact-slice scheme as the Gram products.  The states of Y are first rescaled by powers of two
 // taken from the overlap diagonal (Y~ = Y 2^-d, W~ = 2^d W, so Y~ W~ = Y W and the rows of Y~
 // hold numbers of comparable size); each grid-point row of Y~ is then sliced with its own
-// exponent e_r over all states, each column of W~ with its own exponent f_j.  The contraction
-// runs over the states (K = N), so one int32 accumulation per level covers it exactly, and
-//     psi[r][j] = 2^(e_r + f_j) (acc2 2^-14 + acc3 2^-21 + acc4 2^-28)
-// is formed exactly in FP64 and stored straight into the caller's (unpadded) FP64 layout.
-// The three-slice representation (relative 2^-20 of the row / column maximum, unbiased) makes
-// the rotation as accurate as an FP32 GEMM of the same depth.
+// exponent e_r over all states, each column of W~ with its own exponent f_j (23-bit integers
+// in balanced base-256 digits).  The contraction runs over the states (K = N), so one int32
+// accumulation per level covers it exactly, and
+//     psi[r][j] = 2^(e_r + f_j) (acc0 2^-12 + acc1 2^-20 + acc2 2^-28 + acc3 2^-36)
+// is formed in FP64 and stored straight into the caller's (unpadded) FP64 layout.  Measured
+// against FP64 products of the same data, the rotation is as accurate as an FP32 GEMM of the
+// same depth (about 1e-6 of each state's largest element).
 // ---------------------------------------------------------------------------------------------
 struct RotArgs {
     int N;            // states (K extent and output columns)
@@ -546,6 +559,8 @@ __global__ void __launch_bounds__(kRotThreads, 1)
                 mma_i8(tmem + 256, a[0] + off, b[2] + off, acc);
                 mma_i8(tmem + 256, a[1] + off, b[1] + off, 1u);
                 mma_i8(tmem + 256, a[2] + off, b[0] + off, 1u);
+                mma_i8(tmem + 384, a[1] + off, b[2] + off, acc);
+                mma_i8(tmem + 384, a[2] + off, b[1] + off, 1u);
             }
             mma_commit(&empty[s]);
         }
@@ -573,18 +588,19 @@ __global__ void __launch_bounds__(kRotThreads, 1)
         const uint32_t lb = (uint32_t)(quarter * 32) << 16;
 #pragma unroll 1
         for (int c0 = part * (BN / kRotParts); c0 < (part + 1) * (BN / kRotParts); c0 += 16) {
-            uint32_t r2[16], r3[16], r4[16];
+            uint32_t r2[16], r3[16], r4[16], r5[16];
             tmem_ld16(tmem + lb + (uint32_t)c0, r2);
             tmem_ld16(tmem + lb + 128u + (uint32_t)c0, r3);
             tmem_ld16(tmem + lb + 256u + (uint32_t)c0, r4);
+            tmem_ld16(tmem + lb + 384u + (uint32_t)c0, r5);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (ridx >= 0) {
 #pragma unroll
                 for (int t = 0; t < 16; ++t) {
                     const int j = n0 + c0 + t;
                     if (j < g.N) {
-                        const double x = (double)(int)r2[t] * 0x1p-14 + (double)(int)r3[t] * 0x1p-21 +
-                                         (double)(int)r4[t] * 0x1p-28;
+                        const double x = (double)(int)r2[t] * 0x1p-12 + (double)(int)r3[t] * 0x1p-20 +
+                                         (double)(int)r4[t] * 0x1p-28 + (double)(int)r5[t] * 0x1p-36;
                         g.psi[(long long)j * g.ldp + ridx] = x * rs * fps[c0 + t];  // exact: powers of two
                     }
                 }
@@ -609,7 +625,7 @@ __global__ void colexp_kernel(const double* __restrict__ Ms, int n, int* __restr
     }
 }
 
-// Rows of Y 2^-d -> exponent e_r and three int8 slices a_q[r][i] (state index contiguous,
+// Rows of Y 2^-d -> exponent e_r and three int8 digit slices a_q[r][i] (state index contiguous,
 // row stride ldk >= N, states N..ldk-1 written as zero).  CTA = 32 consecutive rows, all
 // states staged in shared memory [state][row] (row stride 33).
 __global__ void __launch_bounds__(256)
@@ -632,7 +648,7 @@ __global__ void __launch_bounds__(256)
         for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
         int E = 0;
         if (m > 0.0f) frexpf(m, &E);
-        if (lane == 0) es[rr] = (m > 0.0f) ? E + 1 : 0;
+        if (lane == 0) es[rr] = (m > 0.0f) ? E : 0;
     }
     __syncthreads();
     for (int rr = w; rr < 32; rr += 8) {
@@ -640,7 +656,7 @@ __global__ void __launch_bounds__(256)
         if (r >= rows) continue;
         const int e = es[rr];
         if (lane == 0) erow[r] = e;
-        const float sc = pow2f(7 - e);
+        const float sc = pow2f(22 - e);
         for (int i0 = 4 * lane; i0 < ldk; i0 += 128) {
             char4 o1, o2, o3;
             int8_t* p1 = reinterpret_cast<int8_t*>(&o1);
@@ -658,7 +674,8 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// Columns of 2^d W (FP64, column-major N x N) -> exponent f_j and three int8 slices b_q[j][i].
+// Columns of 2^d W (FP64, column-major N x N) -> exponent f_j and three int8 digit slices b_q[j][i]
+// of rint(2^(d_i + 22 - f_j) W_ij).
 __global__ void __launch_bounds__(128)
     slice_w_kernel(int8_t* __restrict__ b1, int8_t* __restrict__ b2, int8_t* __restrict__ b3, long long ldk,
                    double* __restrict__ fpow, const double* __restrict__ W, int N, const int* __restrict__ dcol) {
@@ -674,18 +691,15 @@ __global__ void __launch_bounds__(128)
     m = fmax(fmax(red[0], red[1]), fmax(red[2], red[3]));
     int E = 0;
     if (m > 0.0) frexp(m, &E);
-    const int f = (m > 0.0) ? E + 1 : 0;
+    const int f = (m > 0.0) ? E : 0;
     if (threadIdx.x == 0) fpow[j] = pow2d(f);
     for (int i = threadIdx.x; i < ldk; i += blockDim.x) {
-        double t = (i < N) ? ldexp(col[i], dcol[i] + 7 - f) : 0.0;
-        const double a = rint(t);
-        t = (t - a) * 128.0;
-        const double b = rint(t);
-        t = (t - b) * 128.0;
-        const double c = rint(t);
-        b1[(long long)j * ldk + i] = (int8_t)(int)a;
-        b2[(long long)j * ldk + i] = (int8_t)(int)b;
-        b3[(long long)j * ldk + i] = (int8_t)(int)c;
+        const double t = (i < N) ? ldexp(col[i], dcol[i] + 22 - f) : 0.0;  // |t| < 2^22
+        int8_t a, b, c;
+        digits3(__double2int_rn(t), a, b, c);
+        b1[(long long)j * ldk + i] = a;
+        b2[(long long)j * ldk + i] = b;
+        b3[(long long)j * ldk + i] = c;
     }
 }
 

@@ -37,6 +37,24 @@ int launch_cheb_step(const StencilGeom& g, const T* x, long long ldx, const T* x
                      long long ldout, const S* V, int ncol, double a, double b, double d, const T* phl,
                      const T* phr, cudaStream_t st);
 
+// Centre coefficient of a Chebyshev step, -0.5 a (D2x[0] + D2y[0] + D2z[0]) + b, for neighbour
+// coefficients c[p] = -0.5 a D2[p] stored in precision S, returned as a (hi, lo) pair in S.
+// FP32 (S = float): the centre is moved by the neighbours' rounding, -2 sum (c32 - c64), so the
+// FP32 operator keeps the FP64 row sum (a constant keeps its exact kinetic energy), and it is
+// carried as two floats.  A single float of ~40 Ha is off by up to 1.3e-6 Ha, and so would be
+// every Ritz value of the mixed pass, shifted uniformly.  FP64: hi = the centre, lo = 0.
+template <typename S>
+void centre_coef(const StencilGeom& g, double a, double b, const S* cx, const S* cy, const S* cz, S* hi, S* lo) {
+    double c = -0.5 * a * (g.D2x[0] + g.D2y[0] + g.D2z[0]) + b;
+    if (sizeof(S) == sizeof(float)) {
+        for (int p = 1; p <= g.R; ++p)
+            c -= 2.0 * (((double)cx[p] + 0.5 * a * g.D2x[p]) + ((double)cy[p] + 0.5 * a * g.D2y[p]) +
+                        ((double)cz[p] + 0.5 * a * g.D2z[p]));
+    }
+    *hi = (S)c;
+    *lo = (S)(c - (double)*hi);
+}
+
 // Padded row length used by the pipelined stencil: rows and Veff rows must be 16-byte multiples.
 inline int pipe_row_elems(int nx, size_t scalar_size) {
     const int q = (int)(16 / scalar_size);

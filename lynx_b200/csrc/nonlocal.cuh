@@ -120,7 +120,15 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
     for (int m = 0; m < PJ; ++m) {
         const int j = jq + m * JG;
-        if (j < np) alpha[(long long)(poff + j) * ncolp + n0 + n] = vscale((S)(tab.gamma[poff + j] * dV), acc[m]);
+        if (j < np) {
+            // Gamma dV as an FP32 (hi, lo) pair: a single rounded float would scale the projector's
+            // channel by a fixed 1 + O(6e-8) and shift every Ritz value alike
+            const double gd = tab.gamma[poff + j] * dV;
+            const S hi = (S)gd;
+            T v = vscale(hi, acc[m]);
+            if (sizeof(S) == sizeof(float)) v = fmac(v, (S)(gd - (double)hi), acc[m]);
+            alpha[(long long)(poff + j) * ncolp + n0 + n] = v;
+        }
     }
 }
 
@@ -405,11 +413,17 @@ __global__ void __launch_bounds__(256)
         for (int m = 0; m < NPG; ++m) {
             const int j = pg * NPG + m;
             if (j < np) {
-                const T sc = (T)(tab.gamma[poff + j] * dV);
+                const double gd = tab.gamma[poff + j] * dV;  // applied as a (hi, lo) pair in FP32
+                const T sc = (T)gd;
+                const T sl = (T)(gd - (double)sc);
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const int col = n0 + 4 * cg + k;
-                    if (col < ncolp) alpha[(long long)(poff + j) * ncolp + col] = sc * acc[k][m];
+                    if (col < ncolp) {
+                        T v = sc * acc[k][m];
+                        if (sizeof(T) == sizeof(float)) v = fma(sl, acc[k][m], v);
+                        alpha[(long long)(poff + j) * ncolp + col] = v;
+                    }
                 }
             }
         }

@@ -77,7 +77,7 @@ struct StencilArgs {
     int TY;      // band height = TYT * RY
     int zchunk;  // z-planes per CTA
     S cx[9], cy[9], cz[9];  // cx[p] = -0.5 * a * D2_x[p], p = 1..R
-    S diag;                 // -0.5 * a * (D2_x[0] + D2_y[0] + D2_z[0]) + b
+    S diag, diag_lo;        // -0.5 * a * (D2_x[0] + D2_y[0] + D2_z[0]) + b as a (hi, lo) pair (centre_coef)
     S a;                    // multiplies Veff .* x
     S d;                    // multiplies xold
     T phl[3], phr[3];       // multipliers of left / right ghosts per direction (1, 0 or Bloch phase)
@@ -261,13 +261,17 @@ __global__ void __launch_bounds__(kStencilMaxThreads)
         for (int r = 0; r < RY; ++r) {
             if (!own[r]) continue;
             const T* c = sm + (R + yl[r]) * pitch + tx + R;
-            T acc = vscale(A.diag, w[R][r]);
+            // neighbour sums first, the (large) centre term last, so that the accumulator stays
+            // small where the centre's lo part is added (FP32: no spectrum-wide shift)
+            T acc = vscale(A.cx[1], vadd(c[1], c[-1]));
 #pragma unroll
-            for (int p = 1; p <= R; ++p) acc = fmac(acc, A.cx[p], vadd(c[p], c[-p]));
+            for (int p = 2; p <= R; ++p) acc = fmac(acc, A.cx[p], vadd(c[p], c[-p]));
 #pragma unroll
             for (int p = 1; p <= R; ++p) acc = fmac(acc, A.cy[p], vadd(c[p * pitch], c[-p * pitch]));
 #pragma unroll
             for (int p = 1; p <= R; ++p) acc = fmac(acc, A.cz[p], vadd(w[R + p][r], w[R - p][r]));
+            acc = fmac(acc, A.diag, w[R][r]);
+            if (sizeof(S) == sizeof(float)) acc = fmac(acc, A.diag_lo, w[R][r]);
             acc = fmac(acc, A.a * v_cur[r], w[R][r]);
             if (XOLD) acc = fmac(acc, A.d, xo_cur[r]);
             oc[obase + yl[r] * nx] = acc;

@@ -93,7 +93,7 @@ int launch_cheb_step(const StencilGeom& g, const T* x, long long ldx, const T* x
         A.cy[p] = (S)(-0.5 * a * g.D2y[p]);
         A.cz[p] = (S)(-0.5 * a * g.D2z[p]);
     }
-    A.diag = (S)(-0.5 * a * (g.D2x[0] + g.D2y[0] + g.D2z[0]) + b);
+    centre_coef<S>(g, a, b, A.cx, A.cy, A.cz, &A.diag, &A.diag_lo);
     A.a = (S)a;
     A.d = (S)d;
     for (int k = 0; k < 3; ++k) {

@@ -54,7 +54,7 @@ template <typename T>
 struct PipeCoef {
     using S = typename ScalarOf<T>::type;
     S cx[9], cy[9], cz[9];
-    S diag, a, d;
+    S diag, diag_lo, a, d;  // centre coefficient as a (hi, lo) pair (centre_coef)
     T phl[3], phr[3];
 };
 
@@ -493,11 +493,15 @@ __global__ void __launch_bounds__(MAXT, 1)
                 nl_w = smem_u32(wnl_of(st)) - (uint32_t)walign[st] * 4u;
             }
             const float2 dg = make_float2(C.diag, C.diag);
+            const float2 dgl = make_float2(C.diag_lo, C.diag_lo);
+            // the neighbour sums first and the (large) centre term last: accumulated from the centre
+            // on, the sum would sit at ~40 Ha x, where the rounding loses the centre's lo part and
+            // shifts the whole spectrum
 #pragma unroll
             for (int r = 0; r < RY; ++r) {
-                acc[r] = __fmul2_rn(dg, w[J + R][r]);
+                acc[r] = __fmul2_rn(make_float2(C.cz[1], C.cz[1]), __fadd2_rn(w[J + R + 1][r], w[J + R - 1][r]));
 #pragma unroll
-                for (int p = 1; p <= R; ++p)
+                for (int p = 2; p <= R; ++p)
                     acc[r] = __ffma2_rn(make_float2(C.cz[p], C.cz[p]), __fadd2_rn(w[J + R + p][r], w[J + R - p][r]),
                                         acc[r]);
             }
@@ -554,6 +558,7 @@ __global__ void __launch_bounds__(MAXT, 1)
                         acc[r].y = fmaf(C.cx[p], sr.x, acc[r].y);
                     }
                 }
+                acc[r] = __ffma2_rn(dgl, w[J + R][r], __ffma2_rn(dg, w[J + R][r], acc[r]));
                 const float2 vv = lds<float2>(smem_u32(v_s) + soffb + r * rowbS);
                 acc[r] = __ffma2_rn(__fmul2_rn(make_float2(C.a, C.a), vv), w[J + R][r], acc[r]);
                 if (XOLD) acc[r] = __ffma2_rn(make_float2(C.d, C.d), lds<float2>(smem_u32(xo_s) + yoffb + r * rowb), acc[r]);
@@ -590,10 +595,14 @@ __global__ void __launch_bounds__(MAXT, 1)
 #pragma unroll
         for (int r = 0; r < RY; ++r) {
             const T* wc = reinterpret_cast<const T*>(&w[J + R][r]);
+            {  // neighbour sums first, the centre term last (see the packed path)
+                const T* a_ = reinterpret_cast<const T*>(&w[J + R + 1][r]);
+                const T* b_ = reinterpret_cast<const T*>(&w[J + R - 1][r]);
 #pragma unroll
-            for (int u = 0; u < RX; ++u) acc[r][u] = vscale(C.diag, wc[u]);
+                for (int u = 0; u < RX; ++u) acc[r][u] = vscale(C.cz[1], vadd(a_[u], b_[u]));
+            }
 #pragma unroll
-            for (int p = 1; p <= R; ++p) {
+            for (int p = 2; p <= R; ++p) {
                 const T* a_ = reinterpret_cast<const T*>(&w[J + R + p][r]);
                 const T* b_ = reinterpret_cast<const T*>(&w[J + R - p][r]);
 #pragma unroll
@@ -670,6 +679,8 @@ __global__ void __launch_bounds__(MAXT, 1)
                 const T* xo_e = reinterpret_cast<const T*>(&xo_v);
 #pragma unroll
                 for (int u = 0; u < RX; ++u) {
+                    acc[r][u] = fmac(acc[r][u], C.diag, wc[u]);
+                    if (sizeof(S) == sizeof(float)) acc[r][u] = fmac(acc[r][u], C.diag_lo, wc[u]);
                     acc[r][u] = fmac(acc[r][u], C.a * vv[u], wc[u]);
                     if (XOLD) acc[r][u] = fmac(acc[r][u], C.d, xo_e[u]);
                 }

@@ -229,7 +229,7 @@ int launch_cheb_pipe(const StencilGeom& g, int nxp, const T* x, long long ldx, c
         C.cy[p] = (S)(-0.5 * a * g.D2y[p]);
         C.cz[p] = (S)(-0.5 * a * g.D2z[p]);
     }
-    C.diag = (S)(-0.5 * a * (g.D2x[0] + g.D2y[0] + g.D2z[0]) + b);
+    centre_coef<S>(g, a, b, C.cx, C.cy, C.cz, &C.diag, &C.diag_lo);
     C.a = (S)a;
     C.d = (S)d;
     for (int k = 0; k < 3; ++k) {

@@ -7,7 +7,10 @@ The reference computes these products in FP64 (src/solvers/EigenSolver.cu:195-23
 projection, :312-329 rotation).  Bars:
   * Gram: max_ij |dMs_ij| / sqrt(Ms_ii Ms_jj) <= 1e-7 (upper triangle), and the same for Hs
     with sqrt(Ms_ii |hy_j|^2 scale);
-  * rotation: per state j, max_r |dpsi_rj| / max_r |psi_rj| <= 1e-6.
+  * rotation: per state j, the relative 2-norm error ||dpsi_j|| / ||psi_j|| <= 2e-6 and
+    max_r |dpsi_rj| / max_r |psi_rj| <= 3e-6, and no worse than 4x an FP32 GEMM of the same
+    FP32 data (cuBLAS SGEMM, TF32 off): the rotation is meant to be as accurate as an FP32
+    product of depth N.
 Cases: the Si216 workload's shape (729 088 rows, 520 states: five 128-state tiles with a ragged
 last one, K split into chunks), 129 states (a one-state ragged tile), and a K extent that is not
 a multiple of the 128-row K step.  Column scales span four decades, as the filtered blocks do."""
@@ -86,8 +89,17 @@ def test_rotate_mixed_matches_fp64(ctx, rows, n):
                                          ctypes.c_void_p(Ms.data_ptr()), ctypes.c_void_p(Wc.data_ptr()), n,
                                          ctypes.c_void_p(psi.data_ptr()), rows))
     ref = (Y64.T @ W).T  # psi_ref[j] = sum_i W[i, j] y_i
-    err = ((psi - ref).abs().max(1).values / ref.abs().max(1).values).max().item()
-    assert err <= 1e-6, err
+
+    def errs(p):
+        d = p - ref
+        return ((d.norm(dim=1) / ref.norm(dim=1)).max().item(),
+                (d.abs().max(1).values / ref.abs().max(1).values).max().item())
+
+    e2, emax = errs(psi)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    f2, _ = errs((Y.T @ W.float()).T.double())
+    assert e2 <= 2e-6 and emax <= 3e-6, (e2, emax)
+    assert e2 <= 4.0 * f2, (e2, f2)
 
 
 def test_gram_mixed_flags_nan(ctx):
