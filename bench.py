@@ -40,8 +40,9 @@ METRIC_NOTE = ("value = seconds per CheFSI pass at fixed V_eff (filter + H*Y + R
 # Whole planes stream through the same band geometry at every size, so the traffic of a launch
 # scales with the updates it processes.
 TRAFFIC_PER_UPDATE = {"mixed": 440.271e6 / (216000 * 160), "fp64": 864.076e6 / (216000 * 160)}
-# The same for the launch the pass runs, with the fused nonlocal term (filled from its capture).
-TRAFFIC_PER_UPDATE_FUSED = {"mixed": None, "fp64": None}
+# The same for the launch the pass runs, with the fused nonlocal term: 482.0 MB per FP32 launch at
+# Si64 (dram__bytes_read.sum 369.85 MB + dram__bytes_write.sum 112.16 MB, mean of three launches).
+TRAFFIC_PER_UPDATE_FUSED = {"mixed": 482.0e6 / (216000 * 160), "fp64": None}
 
 CONFIGS = {
     # name: (reps, grid, nstates, degree, displace)

@@ -169,8 +169,8 @@ struct NLDev {
 
 // Column block widths of the nonlocal kernels; alpha rows are padded to a multiple of kNLColBlock.
 constexpr int kNLColBlock = 32;
-// Points per tile (= threads per CTA) of the compact expansion kernel.
-constexpr int kExpTilePts = 256;
+// Points per tile of the compact expansion kernel (128 threads x 4 consecutive points).
+constexpr int kExpTilePts = 512;
 
 template <typename T>
 int launch_nl_gather(const NLDev& nl, const T* x, long long ld, int ncol, T* alpha, int ncolp, double dV,

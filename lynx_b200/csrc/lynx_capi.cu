@@ -215,7 +215,7 @@ struct lynx_ctx {
     DevBuf rwork;           // slices and exponents of the tensor-core rotation
     bool no_tc_gram = false;  // diagnostic switch: FP64 library products for the mixed path
     bool autotune = true;     // time the compiled stencil launch shapes on first use per grid
-    std::map<std::array<long long, 7>, int> pipe_shape;  // chosen launch shape per (type, grid, columns, fused)
+    std::map<std::array<long long, 8>, int> pipe_shape;  // chosen launch shape per (type, grid, columns, fused, xold)
     bool fuse_nl = true;      // add the nonlocal term inside the stencil when the spheres are disjoint
     // with fuse_nl: the stencil also writes compact sphere-point copies of its output and the
     // next step gathers from them (measured slower than the direct gather on B200: off)
@@ -606,8 +606,8 @@ int pipe_launch_tuned(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* 
                       const T* phr, const PipeNLHost* nlh) {
     const StencilGeom g = geom(c);
     const int nsh = pipe_shape_count<T>(g.R);
-    const std::array<long long, 7> key = {(long long)sizeof(T), (long long)ScalarOf<T>::cplx, nxp, c->ny, c->nz,
-                                          ncol, nlh != nullptr};
+    const std::array<long long, 8> key = {(long long)sizeof(T), (long long)ScalarOf<T>::cplx, nxp, c->ny, c->nz,
+                                          ncol, nlh != nullptr, xold != nullptr && d != 0.0};
     auto it = c->pipe_shape.find(key);
     if (it != c->pipe_shape.end() || nsh <= 1 || !c->autotune) {
         const int si = (it != c->pipe_shape.end()) ? it->second : 0;
@@ -617,12 +617,16 @@ int pipe_launch_tuned(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* 
     cudaEvent_t e0, e1;
     LYNX_CUDA_TRY(cudaEventCreate(&e0));
     LYNX_CUDA_TRY(cudaEventCreate(&e1));
-    int best = 0;
+    int best = -1;
     float best_ms = 1e30f;
     int rc = LYNX_OK;
     for (int si = 0; si < nsh && rc == LYNX_OK; ++si) {
         rc = launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
                                     c->errflag.as<int>(), c->stream, si, nlh);
+        if (rc == LYNX_ERR_UNSUPPORTED) {  // this shape's stages do not fit: try the others
+            rc = LYNX_OK;
+            continue;
+        }
         if (rc != LYNX_OK) break;
         cudaEventRecord(e0, c->stream);
         rc = launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
@@ -644,11 +648,14 @@ int pipe_launch_tuned(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != LYNX_OK) return rc;
+    if (best < 0) {
+        set_error("no compiled launch shape of the pipelined stencil fits this grid");
+        return LYNX_ERR_UNSUPPORTED;
+    }
     c->pipe_shape[key] = best;
-    if (best != nsh - 1)  // leave the chosen shape's (identical) output as the result of record
-        return launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
-                                      c->errflag.as<int>(), c->stream, best, nlh);
-    return LYNX_OK;
+    // leave the chosen shape's (identical) output as the result of record
+    return launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
+                                  c->errflag.as<int>(), c->stream, best, nlh);
 }
 
 // Adds the duration of the stencil launch bracketed by c->kt[0] (recorded before it) and an event

@@ -577,59 +577,112 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-// The same expansion with the alpha rows of a tile's atoms staged in shared memory.  CTA = one
-// tile of kExpTilePts consecutive points x one 128-byte column block (CB columns); thread = one
-// point.  Consecutive points in grid order cross several spheres, so the lanes of a warp need
-// different atoms' rows: read from global memory those requests serialise in L1 (the kernel
-// above is L1-bound), from shared memory they do not.  Row r (slot * max_np + j) holds 8 chunks
-// of 16 bytes, chunk q stored at position q ^ (r & 7), so lanes reading different atoms' rows in
-// one instruction hit different banks.  Sums in the order of the kernel above.
-template <typename T>
-__global__ void __launch_bounds__(kExpTilePts)
+// The same expansion, tiled.  CTA = one tile of kExpTilePts consecutive points (grid order) x
+// CBN columns, 128 threads; thread = 4 consecutive points, so its stores of W are 16-byte
+// vectors along the points and a warp writes 512 contiguous bytes per column.  The tile's chi
+// values are staged in shared memory once, and the columns are swept in groups of VW (one
+// 16-byte vector of alpha per (atom, projector)); the alpha vectors of the tile's atoms for the
+// next group are fetched into registers while the current group is computed.  Neighbouring
+// points mostly lie on one atom: a thread reads an alpha vector only where its points change
+// atom, so shared-memory traffic is about a quarter of reading it per point.  NP (>= every
+// atom's projector count) is a compile-time bound, so the projector loop unrolls and its
+// shared-memory loads overlap.  Every (point, column) sums j = 0 .. NP-1 in order from zero
+// (chi is zero past the atom's projector count), the order of the kernel above.
+constexpr int kExpThreads = kExpTilePts / 4;
+template <typename T, int NP>
+__global__ void __launch_bounds__(kExpThreads)
     nl_expand_tile_kernel(T* __restrict__ W, long long ldw, int ncol, int ncolp, int n_pts,
-                          const T* __restrict__ chi_pt, const int2* __restrict__ pt_meta,
-                          const unsigned char* __restrict__ pt_slot, const int* __restrict__ tile_atoms, int amax,
-                          int max_np, const int* __restrict__ atom_poff, const int* __restrict__ atom_nproj,
-                          const T* __restrict__ alpha) {
-    constexpr int VW = 16 / (int)sizeof(T);  // elements per chunk
-    constexpr int CB = 8 * VW;               // columns per CTA
+                          const T* __restrict__ chi_pt, const unsigned char* __restrict__ pt_slot,
+                          const int* __restrict__ tile_atoms, int amax, int max_np, const int* __restrict__ atom_poff,
+                          const int* __restrict__ atom_nproj, const T* __restrict__ alpha) {
+    constexpr int VW = 16 / (int)sizeof(T);  // columns per group (one 16-byte vector)
+    constexpr int NG = 16;                   // groups per CTA
+    constexpr int CBN = NG * VW;             // columns per CTA
+    constexpr int PRE = 1024 / kExpThreads;  // alpha vectors a thread prefetches per group (amax * NP <= 1024)
     extern __shared__ __align__(16) unsigned char smx[];
-    float4* rows = reinterpret_cast<float4*>(smx);
-    const int t = blockIdx.x, n0 = blockIdx.y * CB;
+    T* chi_s = reinterpret_cast<T*>(smx);                                              // [NP][kExpTilePts]
+    float4* al_s = reinterpret_cast<float4*>(smx + (size_t)NP * kExpTilePts * sizeof(T));  // [2][amax * NP]
+    const int t = blockIdx.x, tid = threadIdx.x;
+    const long long p0 = (long long)t * kExpTilePts;
     const int* ta = tile_atoms + (long long)t * amax;
-    for (int e = threadIdx.x; e < amax * max_np * 8; e += blockDim.x) {
-        const int q = e & 7, r = e >> 3;
-        const int slot = r / max_np, j = r - slot * max_np;
-        const int a = ta[slot];
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (a >= 0 && j < atom_nproj[a])
-            v = *reinterpret_cast<const float4*>(alpha + (long long)(atom_poff[a] + j) * ncolp + n0 + q * VW);
-        rows[r * 8 + (q ^ (r & 7))] = v;
+    const int nrow = amax * NP;  // alpha vectors of one group
+    for (int e = tid; e < NP * kExpTilePts; e += kExpThreads) {
+        const int j = e / kExpTilePts, q = e - j * kExpTilePts;
+        const long long m = p0 + q;
+        chi_s[e] = (m < n_pts && j < max_np) ? chi_pt[(long long)j * n_pts + m] : T(0);
     }
-    __syncthreads();
-    const int pt = t * kExpTilePts + threadIdx.x;
-    if (pt >= n_pts) return;
-    const int np = pt_meta[pt].y;
-    const int r0 = (int)pt_slot[pt] * max_np;
-    T acc[CB];
+    // alpha vector r = slot * NP + j of column group g
+    auto fetch = [&](int r, int g) {
+        const int slot = r / NP, j = r - slot * NP;
+        const int a = ta[slot];
+        const int col = blockIdx.y * CBN + g * VW;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (a >= 0 && j < atom_nproj[a] && col < ncolp)
+            v = *reinterpret_cast<const float4*>(alpha + (long long)(atom_poff[a] + j) * ncolp + col);
+        return v;
+    };
+    float4 pre[PRE];
 #pragma unroll
-    for (int k = 0; k < CB; ++k) acc[k] = T(0);
-#pragma unroll 2
-    for (int j = 0; j < np; ++j) {
-        const T c = chi_pt[(long long)j * n_pts + pt];
-        const int r = r0 + j;
+    for (int i = 0; i < PRE; ++i)
+        if (tid + kExpThreads * i < nrow) pre[i] = fetch(tid + kExpThreads * i, 0);
+    const long long m0 = p0 + 4 * tid;
+    int sl[4];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const float4 raw = rows[r * 8 + (q ^ (r & 7))];
-            const T* v = reinterpret_cast<const T*>(&raw);
+    for (int k = 0; k < 4; ++k) sl[k] = (m0 + k < n_pts) ? (int)pt_slot[m0 + k] * NP : 0;
+    for (int g = 0; g < NG; ++g) {
+        const int col0 = blockIdx.y * CBN + g * VW;
+        if (col0 >= ncol) break;
+        float4* al = al_s + (size_t)(g & 1) * nrow;
 #pragma unroll
-            for (int k = 0; k < VW; ++k) acc[q * VW + k] = fma(c, v[k], acc[q * VW + k]);
+        for (int i = 0; i < PRE; ++i)
+            if (tid + kExpThreads * i < nrow) al[tid + kExpThreads * i] = pre[i];
+        __syncthreads();  // the group's alpha vectors (and, at g = 0, the chi tile) are staged
+        if (g + 1 < NG) {
+#pragma unroll
+            for (int i = 0; i < PRE; ++i)
+                if (tid + kExpThreads * i < nrow) pre[i] = fetch(tid + kExpThreads * i, g + 1);
+        }
+        T acc[4][VW];
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int c = 0; c < VW; ++c) acc[k][c] = T(0);
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            T cj[4];
+            const float4* cs = reinterpret_cast<const float4*>(chi_s + (size_t)j * kExpTilePts + 4 * tid);
+#pragma unroll
+            for (int h = 0; h < (int)(4 * sizeof(T) / 16); ++h) reinterpret_cast<float4*>(cj)[h] = cs[h];
+            float4 raw = al[sl[0] + j];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (k > 0 && sl[k] != sl[k - 1]) raw = al[sl[k] + j];
+                const T* v = reinterpret_cast<const T*>(&raw);
+#pragma unroll
+                for (int c = 0; c < VW; ++c) acc[k][c] = fma(cj[k], v[c], acc[k][c]);
+            }
+        }
+        if (m0 + 3 < n_pts) {
+#pragma unroll
+            for (int c = 0; c < VW; ++c)
+                if (col0 + c < ncol) {
+                    T o[4] = {acc[0][c], acc[1][c], acc[2][c], acc[3][c]};
+                    T* dst = W + (long long)(col0 + c) * ldw + m0;
+                    if constexpr (sizeof(T) == 4) {
+                        *reinterpret_cast<float4*>(dst) = *reinterpret_cast<const float4*>(o);
+                    } else {
+                        reinterpret_cast<double2*>(dst)[0] = make_double2(o[0], o[1]);
+                        reinterpret_cast<double2*>(dst)[1] = make_double2(o[2], o[3]);
+                    }
+                }
+        } else {
+#pragma unroll
+            for (int c = 0; c < VW; ++c)
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (col0 + c < ncol && m0 + k < n_pts) W[(long long)(col0 + c) * ldw + m0 + k] = acc[k][c];
         }
     }
-    T* wp = W + (long long)n0 * ldw + pt;
-#pragma unroll
-    for (int k = 0; k < CB; ++k)
-        if (n0 + k < ncol) wp[(long long)k * ldw] = acc[k];
 }
 
 // Nonlocal force reduction for one direction (src/physics/Forces.cpp:772-777, :682-684):

@@ -146,16 +146,24 @@ int launch_nl_expand(const NLDev& nl, T* W, long long ldw, int ncol, const T* al
         const T* chi_pt;
         if constexpr (std::is_same<T, float>::value) chi_pt = nl.chi_pt32;
         else chi_pt = nl.chi_pt64;
-        constexpr int CB = 128 / (int)sizeof(T);  // columns per CTA of the tile kernel
-        static_assert(kNLColBlock % CB == 0, "alpha padding must cover the column blocks");
-        const size_t smem = (size_t)nl.exp_amax * nl.max_np * 128;
-        if (nl.exp_tile_atoms && smem <= 160 * 1024) {
-            dim3 grid((nl.n_pts + kExpTilePts - 1) / kExpTilePts, (ncol + CB - 1) / CB);
-            auto kern = nl_expand_tile_kernel<T>;
-            LYNX_CUDA_TRY(smem_cap(kern, smem));
-            kern<<<grid, kExpTilePts, smem, st>>>(W, ldw, ncol, ncolp, nl.n_pts, chi_pt, nl.pt_meta, nl.pt_slot,
-                                                  nl.exp_tile_atoms, nl.exp_amax, nl.max_np, nl.atom_poff,
-                                                  nl.atom_nproj, alpha);
+        constexpr int CBN = 16 * (16 / (int)sizeof(T));  // columns per CTA of the tile kernel
+        // projector-count bound of the compiled instantiations
+        const int NP = nl.max_np <= 4 ? 4 : nl.max_np <= 9 ? 9 : nl.max_np <= 18 ? 18 : 32;
+        const size_t nrow = (size_t)nl.exp_amax * NP;
+        const size_t smem = (size_t)NP * kExpTilePts * sizeof(T) + 2 * nrow * 16;
+        if (nl.exp_tile_atoms && nrow <= 1024 && smem <= 200 * 1024 && (ldw % 4) == 0) {
+            dim3 grid((nl.n_pts + kExpTilePts - 1) / kExpTilePts, (ncol + CBN - 1) / CBN);
+            auto go = [&](auto kern) -> int {
+                LYNX_CUDA_TRY(smem_cap(kern, smem));
+                kern<<<grid, kExpThreads, smem, st>>>(W, ldw, ncol, ncolp, nl.n_pts, chi_pt, nl.pt_slot,
+                                                      nl.exp_tile_atoms, nl.exp_amax, nl.max_np, nl.atom_poff,
+                                                      nl.atom_nproj, alpha);
+                return LYNX_OK;
+            };
+            if (NP == 4) LYNX_TRY(go(nl_expand_tile_kernel<T, 4>));
+            else if (NP == 9) LYNX_TRY(go(nl_expand_tile_kernel<T, 9>));
+            else if (NP == 18) LYNX_TRY(go(nl_expand_tile_kernel<T, 18>));
+            else LYNX_TRY(go(nl_expand_tile_kernel<T, 32>));
         } else {
             dim3 grid((nl.n_pts + kNL2Pts - 1) / kNL2Pts, (ncol + kNL2Cols - 1) / kNL2Cols);
             nl_expand_pt_kernel<T><<<grid, 256, 0, st>>>(W, ldw, ncol, ncolp, nl.n_pts, chi_pt, nl.pt_meta, alpha);
