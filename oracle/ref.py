@@ -25,6 +25,7 @@ _SIG = {
     "ref_last_error": (ctypes.c_char_p, []),
     "ref_free": (None, []),
     "ref_setup": (_i, [_pd, _i, _i, _i, _i, _i, _i, _pd, ctypes.c_char_p]),
+    "ref_setup_bc": (_i, [_pd, _i, _i, _i, _i, _i, _i, _pd, ctypes.c_char_p, _pi]),
     "ref_nd": (_i, []),
     "ref_dV": (_d, []),
     "ref_stencil": (_i, [_pd] * 12),
@@ -51,6 +52,9 @@ _SIG = {
     "ref_kpoints": (_i, [_i, _i, _i, _pd, _pd, _pd, _pd, _i]),
     "ref_randomize": (None, [_pd, ctypes.c_long, ctypes.c_uint]),
     "ref_set_threads": (_i, [_i]),
+    "ref_nonlocal_force": (_i, [_pd, _pd, _i, _i, _pd, _d, _pd]),
+    "ref_kinetic_nonlocal_stress": (_i, [_pd, _pd, _i, _i, _pd, _d, _pd, _pd]),
+    "ref_density": (_i, [_pd, _pd, _i, _i, _d, _pd]),
 }
 
 _lib = None
@@ -98,8 +102,9 @@ class RefLynx:
         lat = np.ascontiguousarray(cell.latvec, dtype=np.float64)
         pos = np.ascontiguousarray(positions if positions is not None else np.zeros((0, 3)), dtype=np.float64)
         nx, ny, nz = cell.shape
-        _chk(L.ref_setup(_p(lat), 1 if cell.orthogonal else 0, nx, ny, nz, cell.fd_order, len(pos), _p(pos),
-                         (psp8_path or "").encode()))
+        bc = np.ascontiguousarray(getattr(cell, "bc", (0, 0, 0)), dtype=np.int32)
+        _chk(L.ref_setup_bc(_p(lat), 1 if cell.orthogonal else 0, nx, ny, nz, cell.fd_order, len(pos), _p(pos),
+                            (psp8_path or "").encode(), _ip(bc)))
         self.nd = L.ref_nd()
         self.dV = L.ref_dV()
         self.cell = cell
@@ -231,6 +236,45 @@ class RefLynx:
             k = np.ascontiguousarray(kpt, dtype=np.float64)
             _chk(lib().ref_lanczos_kpt(_p(v), _p(lo), _p(hi), tol, maxit, _p(k)))
         return float(lo[0]), float(hi[0])
+
+    # -- consumers of the orbitals (Nspin = 1: occfac = 2; one k-point of weight wk) ----------
+    def _orb_args(self, psi, occ, kpt):
+        cplx = kpt is not None
+        x = self._cols(psi, cplx)
+        o = np.ascontiguousarray(occ, dtype=np.float64)
+        if o.shape[0] != x.shape[1]:
+            raise ValueError("one occupation per orbital column is needed")
+        k = np.ascontiguousarray(kpt if cplx else np.zeros(3), dtype=np.float64)
+        return x, o, k, cplx
+
+    def nonlocal_force(self, psi, occ, kpt=None, wk=1.0):
+        """Forces::compute_nonlocal_cpu (src/physics/Forces.cpp:509-797): n_atom x 3."""
+        x, o, k, cplx = self._orb_args(psi, occ, kpt)
+        n_atom = ctypes.c_int()
+        ni, nt, npj = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _chk(lib().ref_nl_counts(ctypes.byref(ni), ctypes.byref(nt), ctypes.byref(npj), ctypes.byref(n_atom)))
+        f = np.zeros(3 * n_atom.value)
+        _chk(lib().ref_nonlocal_force(x.ctypes.data_as(_pd), _p(o), x.shape[1], int(cplx), _p(k), float(wk), _p(f)))
+        return f.reshape(-1, 3)
+
+    def kinetic_nonlocal_stress(self, psi, occ, kpt=None, wk=1.0):
+        """Stress::compute_nonlocal_kinetic_cpu (src/physics/Stress.cpp:1041-1784), before the
+        division by the cell measure: (stress_k, stress_nl), Voigt xx, xy, xz, yy, yz, zz."""
+        x, o, k, cplx = self._orb_args(psi, occ, kpt)
+        sk = np.zeros(6)
+        snl = np.zeros(6)
+        _chk(lib().ref_kinetic_nonlocal_stress(x.ctypes.data_as(_pd), _p(o), x.shape[1], int(cplx), _p(k), float(wk),
+                                               _p(sk), _p(snl)))
+        return sk, snl
+
+    def density(self, psi, occ, complex_=False, wk=1.0):
+        """ElectronDensity::compute (src/electronic/ElectronDensity.cpp:55-172), Nspin = 1:
+        rho = sum_n 2 wk occ[n] |psi_n|^2."""
+        x = self._cols(psi, complex_)
+        o = np.ascontiguousarray(occ, dtype=np.float64)
+        rho = np.zeros(self.nd)
+        _chk(lib().ref_density(x.ctypes.data_as(_pd), _p(o), x.shape[1], int(complex_), float(wk), _p(rho)))
+        return rho
 
     def kpoints(self, kgrid, shift=(0.0, 0.0, 0.0)):
         n = int(np.prod(kgrid))

@@ -1,4 +1,5 @@
-// Test-oracle harness around the reference LYNX CPU hot path.
+// Test-oracle harness around the reference LYNX CPU hot path (and the forces, stress and density
+// that consume its orbitals).
 //
 // This file is TEST INFRASTRUCTURE.  It is compiled together with the
 // reference's own, unmodified sources (src/solvers/EigenSolver.cpp,
@@ -45,6 +46,13 @@
 #define protected public
 #include "atoms/Crystal.hpp"
 #include "core/Domain.hpp"
+#include "core/LynxContext.hpp"
+#include "electronic/ElectronDensity.hpp"
+#include "electronic/Wavefunction.hpp"
+#include "operators/Gradient.hpp"
+#include "parallel/Parallelization.hpp"
+#include "physics/Forces.hpp"
+#include "physics/Stress.hpp"
 #include "core/FDGrid.hpp"
 #include "core/KPoints.hpp"
 #include "core/Lattice.hpp"
@@ -109,16 +117,18 @@ void ref_free() {
 // reference's Crystal expects (Cartesian for orthogonal cells, non-Cartesian
 // "scaled fractional" for non-orthogonal ones, src/atoms/Crystal.cpp:25-41).
 // psp8_path may be NULL or empty: then no nonlocal projector is set up.
-int ref_setup(const double* latvec, int orth, int Nx, int Ny, int Nz, int fd_order,
-              int natom, const double* pos, const char* psp8_path) {
+// bc: 3 ints, 0 = BCType::Periodic, 1 = BCType::Dirichlet (src/core/types.hpp:14), or NULL
+// for a periodic cell.
+int ref_setup_bc(const double* latvec, int orth, int Nx, int Ny, int Nz, int fd_order,
+                 int natom, const double* pos, const char* psp8_path, const int* bc) {
     return guarded([&] {
         ref_free();
         g = new RefState();
         lynx::Mat3 L;
         for (int i = 0; i < 9; ++i) L.data[i] = latvec[i];
         g->lattice = lynx::Lattice(L, orth ? lynx::CellType::Orthogonal : lynx::CellType::NonOrthogonal);
-        g->grid = lynx::FDGrid(Nx, Ny, Nz, g->lattice, lynx::BCType::Periodic, lynx::BCType::Periodic,
-                               lynx::BCType::Periodic);
+        auto bct = [&](int d) { return (bc && bc[d]) ? lynx::BCType::Dirichlet : lynx::BCType::Periodic; };
+        g->grid = lynx::FDGrid(Nx, Ny, Nz, g->lattice, bct(0), bct(1), bct(2));
         lynx::DomainVertices v;
         v.xs = 0; v.xe = Nx - 1; v.ys = 0; v.ye = Ny - 1; v.zs = 0; v.ze = Nz - 1;
         g->domain = lynx::Domain(g->grid, v);
@@ -148,6 +158,11 @@ int ref_setup(const double* latvec, int orth, int Nx, int Ny, int Nz, int fd_ord
         g->es.domain_ = &g->domain;
         g->es.npband_ = 1;
     });
+}
+
+int ref_setup(const double* latvec, int orth, int Nx, int Ny, int Nz, int fd_order, int natom, const double* pos,
+              const char* psp8_path) {
+    return ref_setup_bc(latvec, orth, Nx, Ny, Nz, fd_order, natom, pos, psp8_path, nullptr);
 }
 
 int ref_nd() { return g ? g->domain.Nd_d() : 0; }
@@ -385,6 +400,101 @@ int ref_kpoints(int kx, int ky, int kz, const double* shift, double* kcart, doub
         w[i] = kp.weights()[i];
     }
     return n;
+}
+
+// ---------------------------------------------------------------------------
+// Nonlocal forces, kinetic / nonlocal stress and the electron density of given orbitals,
+// by the reference's own Forces::compute_nonlocal_cpu (src/physics/Forces.cpp:509-797),
+// Stress::compute_nonlocal_kinetic_cpu (src/physics/Stress.cpp:1041-1784) and
+// ElectronDensity::compute (src/electronic/ElectronDensity.cpp:55-172), for one spin channel
+// (Nspin = 1, so occfac = 2) and one k-point of weight wk (psi complex when is_kpt, at the
+// Cartesian k-point kpt).  The objects those routines read from the LynxContext singleton
+// (gradient, halo, domain, grid, communicators, k-points) are assembled here directly.
+// ---------------------------------------------------------------------------
+namespace {
+// One Wavefunction holding psi (Nd x nband, column-major) and the occupations.
+void fill_wfn(lynx::Wavefunction& w, const double* psi, const double* occ, int nband, bool is_kpt) {
+    const int nd = g->domain.Nd_d();
+    w.allocate(nd, nband, 1, 1, is_kpt);
+    if (is_kpt) {
+        std::memcpy(w.psi_kpt(0, 0).data(), psi, sizeof(Complex) * (size_t)nd * nband);
+    } else {
+        std::memcpy(w.psi(0, 0).data(), psi, sizeof(double) * (size_t)nd * nband);
+    }
+    std::memcpy(w.occupations(0, 0).data(), occ, sizeof(double) * nband);
+}
+// A LynxContext with the pieces Forces::compute_nonlocal_cpu reads (one rank, one spin, one
+// k-point).  Its constructor is private (reachable through the harness's access defines); it is
+// never destroyed, as the reference's destructor finalises MPI and is not linked here.
+lynx::LynxContext* make_context(int nband, const double* kpt) {
+    auto* c = new lynx::LynxContext();
+    c->lattice_.reset(new lynx::Lattice(g->lattice));
+    c->grid_.reset(new lynx::FDGrid(g->grid));
+    c->stencil_.reset(new lynx::FDStencil(g->stencil));
+    lynx::ParallelParams pp;
+    c->parallel_.reset(new lynx::Parallelization(MPI_COMM_WORLD, pp, g->grid, 1, 1, nband));
+    c->parallel_->domain_ = g->domain;
+    c->halo_.reset(new lynx::HaloExchange(g->domain, g->stencil.FDn()));
+    c->gradient_.reset(new lynx::Gradient(g->stencil, g->domain));
+    c->kpoints_.reset(new lynx::KPoints());
+    c->kpoints_->kpts_cart_.assign(1, kpt ? Vec3(kpt[0], kpt[1], kpt[2]) : Vec3(0, 0, 0));
+    c->kpoints_->weights_.assign(1, 1.0);
+    c->scf_bandcomm_ = &c->parallel_->bandcomm();
+    return c;
+}
+}  // namespace
+
+// force: 3 * n_atom doubles (atom-major), the reference's f_nloc_.
+int ref_nonlocal_force(const double* psi, const double* occ, int nband, int is_kpt, const double* kpt, double wk,
+                       double* force) {
+    if (!g || !g->has_vnl) return -1;
+    return guarded([&] {
+        if (is_kpt) g->vnl.set_kpoint(Vec3(kpt[0], kpt[1], kpt[2]));
+        lynx::Wavefunction w;
+        fill_wfn(w, psi, occ, nband, is_kpt != 0);
+        lynx::Forces f;
+        f.ctx_ = make_context(nband, is_kpt ? kpt : nullptr);
+        f.compute_nonlocal_cpu(w, *g->crystal, g->nloc, g->vnl, std::vector<double>(1, wk));
+        std::memcpy(force, f.f_nloc_.data(), sizeof(double) * f.f_nloc_.size());
+    });
+}
+
+// stress_k, stress_nl: 6 doubles each (Voigt xx, xy, xz, yy, yz, zz), before the division by the
+// cell measure (the reference divides by Stress::cell_measure_, set to 1 here).
+int ref_kinetic_nonlocal_stress(const double* psi, const double* occ, int nband, int is_kpt, const double* kpt,
+                                double wk, double* stress_k, double* stress_nl) {
+    if (!g) return -1;
+    return guarded([&] {
+        if (is_kpt && g->has_vnl) g->vnl.set_kpoint(Vec3(kpt[0], kpt[1], kpt[2]));
+        lynx::Wavefunction w;
+        fill_wfn(w, psi, occ, nband, is_kpt != 0);
+        lynx::LynxContext* c = make_context(nband, is_kpt ? kpt : nullptr);
+        lynx::Stress st;
+        st.cell_measure_ = 1.0;
+        lynx::Crystal empty_crystal;
+        const lynx::Crystal& cr = g->has_vnl ? *g->crystal : empty_crystal;
+        std::vector<lynx::AtomNlocInfluence> no_nloc;
+        st.compute_nonlocal_kinetic_cpu(w, cr, g->has_vnl ? g->nloc : no_nloc, g->vnl, c->gradient(), c->halo(),
+                                        c->domain(), c->grid(), std::vector<double>(1, wk), c->scf_bandcomm(),
+                                        c->kpt_bridge(), c->spin_bridge(), &c->kpoints(), 0, 0);
+        std::memcpy(stress_k, st.stress_k_.data(), 6 * sizeof(double));
+        std::memcpy(stress_nl, st.stress_nl_.data(), 6 * sizeof(double));
+    });
+}
+
+// rho: Nd doubles, rho = sum_n 2 wk occ[n] |psi_n|^2 (Nspin = 1).
+int ref_density(const double* psi, const double* occ, int nband, int is_kpt, double wk, double* rho) {
+    if (!g) return -1;
+    return guarded([&] {
+        lynx::Wavefunction w;
+        fill_wfn(w, psi, occ, nband, is_kpt != 0);
+        lynx::LynxContext* c = make_context(nband, nullptr);
+        lynx::ElectronDensity d;
+        d.allocate(g->domain.Nd_d(), 1);
+        d.compute(w, std::vector<double>(1, wk), g->grid.dV(), c->scf_bandcomm(), c->kpt_bridge(), 1, 0, nullptr, 0,
+                  0);
+        std::memcpy(rho, d.rho_total().data(), sizeof(double) * g->domain.Nd_d());
+    });
 }
 
 // Wavefunction::randomize convention (src/electronic/Wavefunction.cpp:53-63).

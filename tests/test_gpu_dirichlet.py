@@ -1,14 +1,16 @@
-"""Dirichlet (zero-ghost) directions on the GPU against the numpy oracle's restatement of the
-reference halo rule (src/parallel/HaloExchange.cpp: non-periodic ghosts stay zero; grid spacing
-L / (N - 1) in those directions).  Mixed boundaries: Dirichlet in x and z, periodic in y.
-Tolerances as for the periodic parity tests: H psi <= 1e-12, FP64 filter <= 1e-10, FP32 filter
-<= 2e-5 per column."""
+"""Dirichlet (zero-ghost) directions on the GPU against the reference's own CPU code built with
+BCType::Dirichlet (oracle/_ref: FDGrid, HaloExchange, Hamiltonian, EigenSolver compiled
+unmodified; src/parallel/HaloExchange.cpp:14-39: non-periodic ghosts stay zero; grid spacing
+L / (N - 1) in those directions) and the numpy oracle's restatement.  Mixed boundaries:
+Dirichlet in x and z, periodic in y.  Tolerances as for the periodic parity tests: H psi <= 1e-12,
+FP64 filter <= 1e-10, FP32 filter <= 2e-5 per column."""
 import numpy as np
 import pytest
 
 from helpers import rel_err
 from lynx_b200 import cell as C
 from oracle import chefsi_oracle as O
+from oracle import ref
 
 pytestmark = pytest.mark.gpu
 
@@ -21,7 +23,8 @@ def dcell():
     V = C.synthetic_veff(cl, pos, noise=1e-3, seed=9)
     op = O.Operator(cl.latvec, cl.shape, order=12, orthogonal=True, bc=cl.bc)
     ctx = solver.Context(cl)
-    return dict(cell=cl, V=V, op=op, ctx=ctx, solver=solver)
+    R = ref.RefLynx(cl)
+    return dict(cell=cl, V=V, op=op, ctx=ctx, solver=solver, R=R)
 
 
 def test_dirichlet_stencil_coefficients(dcell):
@@ -36,6 +39,7 @@ def test_dirichlet_hamiltonian(dcell):
     y_ref = dcell["op"].apply(psi, dcell["V"], 0.3)
     y = dcell["solver"].Hamiltonian(dcell["ctx"], dcell["V"]).apply(psi, shift=0.3)
     assert rel_err(y, y_ref) < 1e-12
+    assert rel_err(y, dcell["R"].h_apply(psi, dcell["V"], 0.3)) < 1e-12
 
 
 def test_dirichlet_filter(dcell):
@@ -46,6 +50,18 @@ def test_dirichlet_filter(dcell):
     es = dcell["solver"].EigenSolver(dcell["ctx"])
     Y = es.chebyshev_filter(X, dcell["V"], lc, lo, hi, 6, precision="fp64")
     assert rel_err(Y, Y_ref) < 1e-10
+    Y_cref = dcell["R"].chebyshev_filter(X, dcell["V"], lc, lo, hi, 6)
+    assert rel_err(Y, Y_cref) < 1e-10
     Ym = es.chebyshev_filter(X, dcell["V"], lc, lo, hi, 6, precision="mixed")
     for j in range(4):
-        assert rel_err(Ym[:, j], Y_ref[:, j]) < 2e-5
+        assert rel_err(Ym[:, j], Y_cref[:, j]) < 2e-5
+
+
+def test_dirichlet_pass_matches_reference(dcell):
+    """One FP64 CheFSI pass with Dirichlet x and z against the reference's EigenSolver::solve."""
+    X = C.random_orbitals(dcell["ctx"].nd, 10, seed=93)
+    lo, hi = dcell["R"].lanczos(dcell["V"])
+    lc = 0.5 * (lo + hi)
+    _, eig_r = dcell["R"].solve(X, dcell["V"], lc, lo, hi, 12)
+    _, eig = dcell["solver"].EigenSolver(dcell["ctx"], "fp64").solve(X, dcell["V"], lc, lo, hi, 12)
+    assert np.abs(eig - eig_r).max() < 1e-9

@@ -1,7 +1,8 @@
-"""GPU nonlocal forces and energy (lynx_nonlocal_force / _kpt) against the numpy oracle of
-src/physics/Forces.cpp:509-797 (itself pinned to a finite difference of the nonlocal energy in
-test_forces_oracle.py), on the same seeded orbitals and projector tables.  FP64: forces within
-1e-10 relative to the largest component, energies within 1e-12 relative."""
+"""GPU nonlocal forces and energy (lynx_nonlocal_force / _kpt) against the reference's own
+Forces::compute_nonlocal_cpu (src/physics/Forces.cpp:509-797, compiled into oracle/_ref) and the
+numpy oracle (for the energy, which that routine does not return), on the same seeded orbitals
+and projector tables.  FP64: forces within 1e-10 relative to the largest component, energies
+within 1e-12 relative."""
 import numpy as np
 import pytest
 
@@ -9,6 +10,7 @@ from helpers import si8_small
 from lynx_b200 import cell as C
 from lynx_b200 import pseudo as P
 from oracle import chefsi_oracle as O
+from oracle import ref
 
 pytestmark = pytest.mark.gpu
 
@@ -36,6 +38,8 @@ def test_nonlocal_force_matches_oracle(synth_psp8, kpt):
     f_ref, e_ref = O.nonlocal_force(psi, occ, _tab(t), st, cl.shape, st["dV"], occfac=2.0, wk=wk, kpt=k,
                                     lengths=cl.lengths)
     f, e = solver.NonlocalProjector(ctx).force(psi, occ, occfac=2.0, kpt=kpt, wk=wk)
-    assert f.shape == f_ref.shape
+    f_cref = ref.RefLynx(cl, pos, synth_psp8).nonlocal_force(psi, occ, kpt=k, wk=wk)
+    assert f.shape == f_cref.shape
+    assert np.abs(f - f_cref).max() <= 1e-10 * np.abs(f_cref).max()
     assert np.abs(f - f_ref).max() <= 1e-10 * np.abs(f_ref).max()
     assert abs(e - e_ref) <= 1e-12 * abs(e_ref)

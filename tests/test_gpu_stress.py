@@ -1,8 +1,9 @@
-"""GPU kinetic and nonlocal stress (lynx_kinetic_nonlocal_stress / _kpt) against the numpy
-oracle of src/physics/Stress.cpp:1041-1784 (itself pinned to finite differences of the kinetic
-and nonlocal energies under strain in test_stress_oracle.py), on the same seeded orbitals and
-projector tables: an orthogonal Si8 cell and the non-orthogonal primitive FCC Si2 cell, Gamma
-point and a Bloch k-point.  FP64 throughout: every component within 1e-10 of the largest
+"""GPU kinetic and nonlocal stress (lynx_kinetic_nonlocal_stress / _kpt) against the reference's
+own Stress::compute_nonlocal_kinetic_cpu (src/physics/Stress.cpp:1041-1784, compiled into
+oracle/_ref; before its division by the cell measure) and the numpy oracle (pinned to finite
+differences of the energies under strain in test_stress_oracle.py), on the same seeded orbitals
+and projector tables: an orthogonal Si8 cell and the non-orthogonal primitive FCC Si2 cell,
+Gamma point and a Bloch k-point.  FP64 throughout: every component within 1e-10 of the largest
 component of its kind."""
 import numpy as np
 import pytest
@@ -11,6 +12,7 @@ from helpers import si8_small
 from lynx_b200 import cell as C
 from lynx_b200 import pseudo as P
 from oracle import chefsi_oracle as O
+from oracle import ref
 
 pytestmark = pytest.mark.gpu
 
@@ -44,6 +46,9 @@ def test_stress_matches_oracle(synth_psp8, kind, kpt):
         ctx.set_kpoint(k)
     sk_ref, snl_ref, _ = O.kinetic_nonlocal_stress(psi, occ, _tab(t), st, cl, st["dV"], occfac=2.0, wk=wk, kpt=k)
     sk, snl = solver.NonlocalProjector(ctx).stress(psi, occ, occfac=2.0, kpt=kpt, wk=wk)
+    sk_c, snl_c = ref.RefLynx(cl, pos, synth_psp8).kinetic_nonlocal_stress(psi, occ, kpt=k, wk=wk)
+    assert np.abs(sk - sk_c).max() <= 1e-10 * np.abs(sk_c).max()
+    assert np.abs(snl - snl_c).max() <= 1e-10 * np.abs(snl_c).max()
     assert np.abs(sk - sk_ref).max() <= 1e-10 * np.abs(sk_ref).max()
     assert np.abs(snl - snl_ref).max() <= 1e-10 * np.abs(snl_ref).max()
     assert np.abs(snl_ref).max() > 0
