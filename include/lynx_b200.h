@@ -262,6 +262,28 @@ LYNX_API int lynx_gram_mixed(lynx_ctx* ctx, const float* Y, const float* HY, lon
 LYNX_API int lynx_rotate_mixed(lynx_ctx* ctx, const float* Y, long long ld, long long rows, const double* Ms,
                                const double* W, int n, double* psi, long long ldp);
 
+/* Electron density of one (spin, k-point) block of device orbitals psi (nband columns, stride ld;
+ * complex interleaved when is_complex): rho[i] = (accumulate ? rho[i] : 0)
+ * + sum_n weight * occ[n] * |psi_n(i)|^2, states with occ[n] < 1e-16 skipped; occ: host, nband
+ * doubles; rho: device, Nd doubles; weight = spin factor (2 for one spin channel) x k-point weight.
+ * Replaces ElectronDensity::compute for one (spin, k-point) (src/electronic/ElectronDensity.cpp:85-121);
+ * the sum over spins and k-points is accumulate = 1 on later blocks. */
+LYNX_API int lynx_electron_density(lynx_ctx* ctx, const double* psi, int nband, int ld, const double* occ,
+                                   double weight, double* rho, int is_complex, int accumulate);
+
+/* One CheFSI pass of real orbitals, as lynx_eigensolver_solve, for a system of one spin channel and
+ * one k-point, followed by the next steps of the SCF iteration on its Ritz values: the Fermi level
+ * (Brent on sum_n weight f(eig_n - Ef) = nelectron, smearing as lynx_fermi_level), the
+ * occupations, and the electron density rho (device, Nd doubles) = sum_n weight f_n |psi_n|^2 of
+ * the new orbitals.  In the mixed-precision pass the tensor-core rotation accumulates the density
+ * from the FP64 orbitals as it writes them, so they are not read again.  *ef_out (may be NULL)
+ * receives Ef.  Replaces, for one (spin, k-point), EigenSolver::solve -> Occupation::compute ->
+ * ElectronDensity::compute in SCF::run (src/physics/SCF.cpp:251-252,433-435). */
+LYNX_API int lynx_eigensolver_solve_density(lynx_ctx* ctx, double* psi, double* eig, const double* veff, int nband,
+                                            int ld, double lambda_cutoff, double eigmin, double eigmax, int degree,
+                                            int precision, double* lambda_cutoff_out, double nelectron, double beta,
+                                            int smearing, double weight, double* rho, double* ef_out);
+
 /* Diagnostic, no counterpart in the reference: one CTA waits, with at most `spins` tries
  * (1 .. 2^20), for an mbarrier phase that nothing completes, with the same bounded wait the
  * pipelined kernels use for their copies.  The wait gives up and the kernel returns; the call

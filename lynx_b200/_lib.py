@@ -87,6 +87,10 @@ _SIGNATURES = {
     "lynx_rotate_mixed": (_c_int, [_p, _p, ctypes.c_longlong, ctypes.c_longlong, _p, _p, _c_int, _p,
                                    ctypes.c_longlong]),
     "lynx_selftest_wait_timeout": (_c_int, [_p, _c_int]),
+    "lynx_electron_density": (_c_int, [_p, _p, _c_int, _c_int, _pd, _c_double, _p, _c_int, _c_int]),
+    "lynx_eigensolver_solve_density": (_c_int, [_p, _p, _pd, _p, _c_int, _c_int, _c_double, _c_double, _c_double,
+                                                _c_int, _c_int, _pd, _c_double, _c_double, _c_int, _c_double, _p,
+                                                _pd]),
 }
 
 EXPORTED = tuple(_SIGNATURES)

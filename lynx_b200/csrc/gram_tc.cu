@@ -477,6 +477,11 @@ struct RotArgs {
     double* psi;      // output, column stride ldp, unpadded rows
     long long ldp;
     int* err;
+    // optional electron density of the rotated orbitals: dens_w[j] = weight * occupation of
+    // state j; this tile's share sum_j dens_w[j] psi[r][j]^2 goes to dens_part[tn * npts + r]
+    const double* dens_w;
+    double* dens_part;
+    long long npts;
 };
 
 __global__ void __launch_bounds__(kRotThreads, 1)
@@ -573,8 +578,14 @@ __global__ void __launch_bounds__(kRotThreads, 1)
     // Epilogue on all warps: warp w reads TMEM lane quarter w % 4 (its 32 rows) and the column
     // part w / 4 of kRotParts, so the stores of several warps per quarter are in flight.
     __shared__ double fps[BN];  // column scales of this tile
-    if (threadIdx.x < BN) fps[threadIdx.x] = (n0 + (int)threadIdx.x < g.N) ? g.fpow[n0 + threadIdx.x] : 0.0;
+    __shared__ double dws[BN];  // density weights of this tile's states
+    __shared__ double dpart[kRotParts][BM];
+    if (threadIdx.x < BN) {
+        fps[threadIdx.x] = (n0 + (int)threadIdx.x < g.N) ? g.fpow[n0 + threadIdx.x] : 0.0;
+        dws[threadIdx.x] = (g.dens_w && n0 + (int)threadIdx.x < g.N) ? g.dens_w[n0 + threadIdx.x] : 0.0;
+    }
     __syncthreads();
+    double dsum = 0.0;  // this thread's row, its part's columns: sum_j w_j psi^2, j in order
     if (ok) {
         const int quarter = warp & 3, part = warp >> 2;
         const long long row = (long long)m0 + quarter * 32 + lane;
@@ -601,8 +612,28 @@ __global__ void __launch_bounds__(kRotThreads, 1)
                     if (j < g.N) {
                         const double x = (double)(int)r2[t] * 0x1p-12 + (double)(int)r3[t] * 0x1p-20 +
                                          (double)(int)r4[t] * 0x1p-28 + (double)(int)r5[t] * 0x1p-36;
-                        g.psi[(long long)j * g.ldp + ridx] = x * rs * fps[c0 + t];  // exact: powers of two
+                        const double v = x * rs * fps[c0 + t];  // exact: powers of two
+                        g.psi[(long long)j * g.ldp + ridx] = v;
+                        if (g.dens_w) dsum = fma(dws[c0 + t] * v, v, dsum);
                     }
+                }
+            }
+        }
+    }
+    if (g.dens_w) {
+        // the four column parts of each row in order, then one partial per (column tile, row)
+        const int quarter = warp & 3, part = warp >> 2;
+        dpart[part][quarter * 32 + lane] = dsum;
+        __syncthreads();
+        if (threadIdx.x < BM) {
+            const long long row = (long long)m0 + threadIdx.x;
+            if (row < g.rows) {
+                const long long xr = row % g.nxp, rest = row / g.nxp;
+                if (xr < g.nx) {
+                    double t = 0.0;
+#pragma unroll
+                    for (int q = 0; q < kRotParts; ++q) t += dpart[q][threadIdx.x];
+                    g.dens_part[(long long)tn * g.npts + xr + (long long)g.nx * rest] = t;
                 }
             }
         }
@@ -792,9 +823,20 @@ int launch_colexp(const double* Ms, int n, void* work, const RotPlan& p, long lo
     return LYNX_OK;
 }
 
+// rho[r] (+)= sum over the column tiles t of part[t * npts + r], in tile order.
+__global__ void dens_tiles_reduce_kernel(double* __restrict__ rho, const double* __restrict__ part, int ntiles,
+                                         long long npts, int accumulate) {
+    for (long long r = blockIdx.x * (long long)blockDim.x + threadIdx.x; r < npts;
+         r += (long long)gridDim.x * blockDim.x) {
+        double s = accumulate ? rho[r] : 0.0;
+        for (int t = 0; t < ntiles; ++t) s += part[(long long)t * npts + r];
+        rho[r] = s;
+    }
+}
+
 int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp, const double* W, int n,
                   const RotPlan& p, void* work, size_t work_bytes, double* psi, long long ldp, int* err,
-                  cudaStream_t st) {
+                  cudaStream_t st, const RotDensity* dens) {
     if (work_bytes < p.work_bytes || (reinterpret_cast<uintptr_t>(work) & 255) || !rot_supported(n)) {
         set_error("rotation workspace too small or misaligned, or too many states for the tensor-core rotation");
         return LYNX_ERR_BAD_ARG;
@@ -827,11 +869,20 @@ int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp
     g.psi = psi;
     g.ldp = ldp;
     g.err = err;
+    g.dens_w = dens ? dens->w : nullptr;
+    g.dens_part = dens ? dens->part : nullptr;
+    g.npts = dens ? dens->npts : 0;
     const size_t smem = STAGES * STAGE_BYTES + 1024 + 256;
     LYNX_CUDA_TRY(smem_cap(rot_i8_kernel, smem));
     const long long ntm = (rows + BM - 1) / BM;
     rot_i8_kernel<<<(unsigned)(ntm * g.ntn), kRotThreads, smem, st>>>(m[0], m[1], m[2], m[3], m[4], m[5], g);
     count_launch();
+    if (dens) {
+        const int blocks = (int)std::min<long long>((dens->npts + 255) / 256, 148LL * 8);
+        dens_tiles_reduce_kernel<<<blocks, 256, 0, st>>>(dens->rho, dens->part, g.ntn, dens->npts,
+                                                         dens->accumulate ? 1 : 0);
+        count_launch();
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("rotation kernel launch failed: %s", cudaGetErrorString(e));

@@ -110,9 +110,23 @@ struct RotPlan {
 RotPlan rot_plan(long long rows, int n);
 bool rot_supported(int n);
 int launch_colexp(const double* Ms, int n, void* work, const RotPlan& p, long long rows, cudaStream_t st);
+// Electron density from the rotation's epilogue: rho[r] (+)= sum_j w[j] psi[r][j]^2 over the
+// npts unpadded grid points, with the per-column-tile partials in part (ceil(n / 128) * npts
+// doubles) reduced in tile order.
+struct RotDensity {
+    const double* w;  // [n] weights (device)
+    double* part;
+    double* rho;      // [npts] (device)
+    long long npts;
+    bool accumulate;
+};
 int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp, const double* W, int n,
                   const RotPlan& p, void* work, size_t work_bytes, double* psi, long long ldp, int* err,
-                  cudaStream_t st);
+                  cudaStream_t st, const RotDensity* dens = nullptr);
+// rho[i] (+)= sum_n w[n] |psi[n * ld + i]|^2 over nd points (T = double or double2; w device).
+template <typename T>
+int launch_density(const T* psi, long long ld, long long nd, int ncol, const double* w, double* rho, bool accumulate,
+                   cudaStream_t st);
 
 // Launches issued by the library (diagnostic counter, incremented by every launcher).
 void count_launch(int n = 1);

@@ -151,6 +151,41 @@ __global__ void hermitize_kernel(double2* A, int N) {
     }
 }
 
+// Electron density of one (spin, k-point) block: rho[i] (+)= sum_n w[n] |psi_n(i)|^2, the states in
+// order (src/electronic/ElectronDensity.cpp:85-121, with w[n] = spin factor * k weight * f_n and
+// w[n] = 0 where the reference skips f_n < 1e-16).  One thread per grid point: the reads of every
+// column are coalesced, and the sum has a fixed order.
+__device__ __forceinline__ double abs2(double v) { return v * v; }
+__device__ __forceinline__ double abs2(double2 v) { return v.x * v.x + v.y * v.y; }
+template <typename T>
+__global__ void density_kernel(const T* __restrict__ psi, long long ld, long long nd, int ncol,
+                               const double* __restrict__ w, double* __restrict__ rho, int accumulate) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nd;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s = accumulate ? rho[i] : 0.0;
+        for (int n = 0; n < ncol; ++n) {
+            const double wn = w[n];
+            if (wn != 0.0) s = fma(wn, abs2(psi[(long long)n * ld + i]), s);
+        }
+        rho[i] = s;
+    }
+}
+
+template <typename T>
+int launch_density(const T* psi, long long ld, long long nd, int ncol, const double* w, double* rho, bool accumulate,
+                   cudaStream_t st) {
+    if (nd <= 0) return LYNX_OK;
+    const int blocks = (int)std::min<long long>((nd + 255) / 256, 148LL * 16);
+    density_kernel<T><<<blocks, 256, 0, st>>>(psi, ld, nd, ncol, w, rho, accumulate ? 1 : 0);
+    count_launch();
+    LYNX_CUDA_TRY(cudaGetLastError());
+    return LYNX_OK;
+}
+template int launch_density<double>(const double*, long long, long long, int, const double*, double*, bool,
+                                    cudaStream_t);
+template int launch_density<double2>(const double2*, long long, long long, int, const double*, double*, bool,
+                                     cudaStream_t);
+
 // Sets *flag when an entry of the N x N column-major matrix A is NaN or Inf (comps doubles per
 // entry: 1 real, 2 complex; upper: only entries on or above the diagonal are valid).
 __global__ void nonfinite_kernel(const double* __restrict__ A, int N, int comps, int upper, int* __restrict__ flag) {
@@ -243,6 +278,14 @@ struct lynx_ctx {
     std::vector<int> h_img_ndc, h_img_atom, h_atom_nproj;
     std::vector<double> h_chi;
     DevBuf sbuf[4];  // stress: third gradient block, chi weighted by x, y, z relative positions
+    // lynx_eigensolver_solve_density: the density request of the current pass
+    struct DensityReq {
+        bool on = false, done = false;
+        double nelectron = 0, beta = 0, weight = 0, ef = 0;
+        int smearing = 0;
+        double* rho = nullptr;
+    } dens;
+    DevBuf dens_w, dens_part;
     // lynx_time_filter_step with with_nonlocal = 2: events around the stencil kernel alone
     bool time_stencil = false;
     cudaEvent_t kt[2] = {nullptr, nullptr};
@@ -1004,6 +1047,20 @@ int rayleigh_ritz_real(lynx_ctx* c, const double* Y, long long ldY, const double
     return rr_subspace_real(c, Y, ldY, psi, ldp, N, eig_host);
 }
 
+// Fermi level of this pass's Ritz values (Occupation::find_fermi_level for one spin and one
+// k-point, every state weighted by the request's weight) and the density weights
+// w[n] = weight * f_n on the device (0 where f_n < 1e-16, which the reference skips).
+int density_weights(lynx_ctx* c, const double* eig, int N) {
+    std::vector<double> wt(N, c->dens.weight), occ(N);
+    LYNX_TRY(lynx_fermi_level(eig, wt.data(), N, c->dens.nelectron, c->dens.beta, c->dens.smearing, &c->dens.ef));
+    LYNX_TRY(lynx_occupations(eig, N, c->dens.ef, c->dens.beta, c->dens.smearing, occ.data()));
+    for (int n = 0; n < N; ++n) wt[n] = (occ[n] < 1e-16) ? 0.0 : c->dens.weight * occ[n];
+    LYNX_TRY(c->dens_w.ensure(sizeof(double) * N));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(c->dens_w.p, wt.data(), sizeof(double) * N, cudaMemcpyHostToDevice, c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));  // wt is a host temporary
+    return LYNX_OK;
+}
+
 // Mixed precision, real: Gram products and rotation of the FP32 blocks on the tensor cores
 // (exact int8 slice products, FP64 combination), subspace algebra in FP64.  More states than
 // the rotation kernel stages take the rotation by DGEMM on an FP64 copy of Y.
@@ -1021,6 +1078,20 @@ int rayleigh_ritz_mixed_real(lynx_ctx* c, const float* Y32, const float* HY32, l
         LYNX_TRY(c->rwork.ensure(rp.work_bytes));
         LYNX_TRY(launch_colexp(c->Ms.as<double>(), N, c->rwork.p, rp, ldb, c->stream));
         LYNX_TRY(rr_small_real(c, N));
+        if (c->dens.on) {
+            // The Ritz values first (checked as after any pass): their occupations weight the
+            // density, which the rotation accumulates from the FP64 orbitals it writes.
+            LYNX_TRY(finish_rr(c, N, eig_host));
+            LYNX_TRY(density_weights(c, eig_host, N));
+            const int ntn = (N + 127) / 128;
+            LYNX_TRY(c->dens_part.ensure(sizeof(double) * (size_t)ntn * c->Nd));
+            RotDensity rd{c->dens_w.as<double>(), c->dens_part.as<double>(), c->dens.rho, c->Nd, false};
+            LYNX_TRY(launch_rot_i8(Y32, ldb, ldb, c->nx, nxp, c->Hs.as<double>(), N, rp, c->rwork.p, c->rwork.bytes,
+                                   psi, ldp, c->errflag.as<int>(), c->stream, &rd));
+            c->dens.done = true;
+            LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+            return LYNX_OK;
+        }
         LYNX_TRY(launch_rot_i8(Y32, ldb, ldb, c->nx, nxp, c->Hs.as<double>(), N, rp, c->rwork.p, c->rwork.bytes, psi,
                                ldp, c->errflag.as<int>(), c->stream));
         return finish_rr(c, N, eig_host);
@@ -2365,6 +2436,56 @@ extern "C" int lynx_selftest_wait_timeout(lynx_ctx* c, int spins) {
     count_launch();
     LYNX_CUDA_TRY(cudaGetLastError());
     return check_errflag(c);
+}
+
+extern "C" int lynx_electron_density(lynx_ctx* c, const double* psi, int nband, int ld, const double* occ,
+                                     double weight, double* rho, int is_complex, int accumulate) {
+    LYNX_CHECK_ARG(c && psi && occ && rho, "null pointer");
+    LYNX_CHECK_ARG(nband > 0, "nband must be positive");
+    const long long l = ld > 0 ? ld : c->Nd;
+    LYNX_CHECK_ARG(l >= c->Nd, "ld < Nd");
+    LYNX_TRY(activate(c));
+    std::vector<double> w(nband);
+    for (int n = 0; n < nband; ++n) w[n] = (occ[n] < 1e-16) ? 0.0 : weight * occ[n];
+    LYNX_TRY(c->dens_w.ensure(sizeof(double) * nband));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(c->dens_w.p, w.data(), sizeof(double) * nband, cudaMemcpyHostToDevice, c->stream));
+    if (is_complex)
+        LYNX_TRY(launch_density<double2>(reinterpret_cast<const double2*>(psi), l, c->Nd, nband,
+                                         c->dens_w.as<double>(), rho, accumulate != 0, c->stream));
+    else
+        LYNX_TRY(launch_density<double>(psi, l, c->Nd, nband, c->dens_w.as<double>(), rho, accumulate != 0,
+                                        c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));  // w is a host temporary
+    return LYNX_OK;
+}
+
+extern "C" int lynx_eigensolver_solve_density(lynx_ctx* c, double* psi, double* eig, const double* veff, int nband,
+                                              int ld, double lc, double emin, double emax, int degree, int precision,
+                                              double* lc_out, double nelectron, double beta, int smearing,
+                                              double weight, double* rho, double* ef_out) {
+    LYNX_CHECK_ARG(c && rho, "null pointer");
+    LYNX_CHECK_ARG(beta > 0 && weight > 0 && nelectron > 0, "nelectron, beta and weight must be positive");
+    c->dens = lynx_ctx::DensityReq();
+    c->dens.on = true;
+    c->dens.nelectron = nelectron;
+    c->dens.beta = beta;
+    c->dens.smearing = smearing;
+    c->dens.weight = weight;
+    c->dens.rho = rho;
+    int st = solve_impl<double, float>(c, psi, eig, veff, nband, ld, lc, emin, emax, degree, precision, lc_out, false);
+    const bool fused = c->dens.done;
+    c->dens.on = false;
+    if (st != LYNX_OK) return st;
+    if (!fused) {  // FP64 pass (or more states than the tensor-core rotation takes): separate kernel
+        std::vector<double> wt(nband, weight), occ(nband);
+        double ef = 0.0;
+        LYNX_TRY(lynx_fermi_level(eig, wt.data(), nband, nelectron, beta, smearing, &ef));
+        LYNX_TRY(lynx_occupations(eig, nband, ef, beta, smearing, occ.data()));
+        c->dens.ef = ef;
+        LYNX_TRY(lynx_electron_density(c, psi, nband, ld, occ.data(), weight, rho, 0, 0));
+    }
+    if (ef_out) *ef_out = c->dens.ef;
+    return LYNX_OK;
 }
 
 extern "C" int lynx_nonlocal_apply_noalloc(lynx_ctx* c, const double* psi, double* hpsi, int ncol, int ld) {

@@ -371,6 +371,26 @@ def occupations(eigs, ef: float, beta: float, smearing: str = "fermi-dirac") -> 
     return occ
 
 
+def electron_density(ctx: Context, psi, occ, weight: float = 2.0, rho=None, complex_: bool = False):
+    """ElectronDensity::compute for one (spin, k-point) block (lynx_electron_density):
+    rho (+)= sum_n weight occ[n] |psi_n|^2.  psi: host (Nd, nband) or device (nband, Nd);
+    rho: a device tensor of Nd doubles to accumulate into, or None for a new one.  Returns rho
+    (a torch CUDA tensor)."""
+    torch = _torch()
+    ctx.sync_stream()
+    a = _DeviceArgs(ctx, psi, complex_)
+    occ = np.ascontiguousarray(occ, dtype=np.float64)
+    if occ.shape[0] != a.ncol:
+        raise ValueError("one occupation per orbital column is needed")
+    acc = rho is not None
+    if rho is None:
+        rho = torch.empty(ctx.nd, dtype=torch.float64, device=f"cuda:{ctx.device}")
+    check(ctx.lib.lynx_electron_density(ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), a.ncol, ctx.nd, dptr(occ),
+                                        float(weight), ctypes.c_void_p(_dev_ptr(rho)), 1 if complex_ else 0,
+                                        1 if acc else 0))
+    return rho
+
+
 def randomize_orbitals(ctx: Context, nband: int, seed: int, complex_: bool = False):
     """Device start orbitals as EigenSolver::randomize_psi_gpu draws them (cuRAND default
     generator, uniform (0, 1], seed as given): a torch tensor (nband, Nd), float64 or complex128
