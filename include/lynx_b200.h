@@ -315,8 +315,12 @@ LYNX_API int lynx_nonlocal_apply_noalloc(lynx_ctx* ctx, const double* psi, doubl
  *                            rotation on the tensor cores (exact int8 slices, as accurate as
  *                            FP64 products of the FP32 blocks to about 1e-8); 0 runs them as FP64
  *                            library products on FP64 copies of the FP32 blocks (slower).
+ *   LYNX_OPT_COMPACT_GATHER: with the fused nonlocal term, 1 makes every filter step also write
+ *                            its output at the sphere points as a compact block, and the next
+ *                            step's projections read that block instead of the full grid; 0
+ *                            (default) reads the full grid.  Same results, bitwise.
  */
-enum { LYNX_OPT_AUTOTUNE = 1, LYNX_OPT_FUSE_NONLOCAL = 2, LYNX_OPT_TC_RAYLEIGH_RITZ = 3 };
+enum { LYNX_OPT_AUTOTUNE = 1, LYNX_OPT_FUSE_NONLOCAL = 2, LYNX_OPT_TC_RAYLEIGH_RITZ = 3, LYNX_OPT_COMPACT_GATHER = 4 };
 LYNX_API int lynx_set_option(lynx_ctx* ctx, int option, int value);
 
 /* Number of kernel launches this library issued since the last reset (diagnostic counter). */

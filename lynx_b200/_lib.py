@@ -16,6 +16,7 @@ LYNX_ERR_BAD_ARG = 1
 OPT_AUTOTUNE = 1
 OPT_FUSE_NONLOCAL = 2
 OPT_TC_RAYLEIGH_RITZ = 3
+OPT_COMPACT_GATHER = 4
 LYNX_ERR_CUDA = 2
 LYNX_ERR_OOM = 3
 LYNX_ERR_CHOL_FAIL = 4

@@ -2382,6 +2382,7 @@ extern "C" int lynx_set_option(lynx_ctx* c, int option, int value) {
         case LYNX_OPT_AUTOTUNE: c->autotune = value != 0; return LYNX_OK;
         case LYNX_OPT_FUSE_NONLOCAL: c->fuse_nl = value != 0; return LYNX_OK;
         case LYNX_OPT_TC_RAYLEIGH_RITZ: c->no_tc_gram = value == 0; return LYNX_OK;
+        case LYNX_OPT_COMPACT_GATHER: c->fuse_compact_gather = value != 0; return LYNX_OK;
         default: set_error("unknown option %d", option); return LYNX_ERR_BAD_ARG;
     }
 }

@@ -685,6 +685,127 @@ __global__ void __launch_bounds__(kExpThreads)
     }
 }
 
+// The same expansion with the projector values in registers and alpha in shared memory.
+// CTA = one tile of kExpTilePts consecutive points (grid order) x kExpRegCols columns; thread =
+// PTS consecutive points (one 16-byte vector of W per column: 4 floats or 2 doubles), whose chi
+// values it loads once into registers.  The alpha rows of the tile's atoms for the CTA's columns
+// are staged in shared memory with one barrier, [slot][projector][column]; the thread then
+// sweeps the columns in groups of VW (one 16-byte alpha vector per projector, re-read only where
+// its points change atom, so one shared-memory load serves up to PTS x VW outputs) and writes W
+// as 16-byte vectors (a warp writes 512 contiguous bytes per column).  Every (point, column)
+// sums j = 0 .. NP-1 in order from zero with fma (chi and alpha are zero past the atom's
+// projector count), the order of the kernels above: bitwise their results.  FP32 column pairs
+// use packed fma.rn.f32x2, element for element the same rounding.
+constexpr int kExpRegCols = 32;
+template <typename T>
+constexpr int exp_reg_threads() {
+    return kExpTilePts / (16 / (int)sizeof(T));
+}
+template <typename T, int NP>
+__global__ void __launch_bounds__(exp_reg_threads<T>())
+    nl_expand_reg_kernel(T* __restrict__ W, long long ldw, int ncol, int ncolp, int n_pts, int max_np,
+                         const T* __restrict__ chi_pt, const unsigned char* __restrict__ pt_slot,
+                         const int* __restrict__ tile_atoms, int amax, const int* __restrict__ atom_poff,
+                         const int* __restrict__ atom_nproj, const T* __restrict__ alpha) {
+    constexpr int PTS = 16 / (int)sizeof(T);   // points per thread
+    constexpr int VW = 16 / (int)sizeof(T);    // columns per alpha vector
+    constexpr int NV = kExpRegCols / VW;       // alpha vectors per (slot, projector) row
+    constexpr int NT = exp_reg_threads<T>();
+    constexpr bool kF32 = std::is_same<T, float>::value;
+    using V16 = typename std::conditional<kF32, float4, double2>::type;
+    extern __shared__ __align__(16) unsigned char smx[];
+    // [amax][NP][NV] with the slot stride padded by one vector: the points of a warp span several
+    // atoms (runs of ~8 points alternate between atoms along a row), and unpadded slot rows would
+    // all start on the same banks
+    constexpr int SS = NP * NV + 1;
+    V16* al_s = reinterpret_cast<V16*>(smx);
+    const int t = blockIdx.x, tid = threadIdx.x;
+    const int c0 = blockIdx.y * kExpRegCols;
+    const int* ta = tile_atoms + (long long)t * amax;
+    for (int e = tid; e < amax * NP * NV; e += NT) {
+        const int r = e / NV, v = e - r * NV;
+        const int slot = r / NP, j = r - slot * NP;
+        const int a = ta[slot];
+        const int col = c0 + v * VW;
+        V16 val;
+        T* vp = reinterpret_cast<T*>(&val);
+#pragma unroll
+        for (int c = 0; c < VW; ++c) vp[c] = T(0);
+        if (a >= 0 && j < atom_nproj[a] && col < ncolp)
+            val = *reinterpret_cast<const V16*>(alpha + (long long)(atom_poff[a] + j) * ncolp + col);
+        al_s[slot * SS + j * NV + v] = val;
+    }
+    const long long m0 = (long long)t * kExpTilePts + PTS * tid;
+    const int npt = (int)max(0LL, min((long long)PTS, (long long)n_pts - m0));
+    T cj[NP][PTS];
+    const bool vec = npt == PTS && (n_pts % PTS) == 0;  // chi rows 16-byte aligned at m0
+#pragma unroll
+    for (int j = 0; j < NP; ++j) {
+        const T* src = chi_pt + (long long)j * n_pts + m0;
+        if (j < max_np && vec) {
+            const V16 q = *reinterpret_cast<const V16*>(src);
+            const T* qp = reinterpret_cast<const T*>(&q);
+#pragma unroll
+            for (int k = 0; k < PTS; ++k) cj[j][k] = qp[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < PTS; ++k) cj[j][k] = (j < max_np && k < npt) ? src[k] : T(0);
+        }
+    }
+    int so[PTS];  // each point's slot row in al_s (past the last point: the previous one's)
+#pragma unroll
+    for (int k = 0; k < PTS; ++k) so[k] = (k < npt) ? (int)pt_slot[m0 + k] * SS : (k > 0 ? so[k - 1] : 0);
+    __syncthreads();  // alpha staged
+    if (npt == 0) return;
+#pragma unroll 1
+    for (int g = 0; g < NV; ++g) {
+        const int col = c0 + g * VW;
+        if (col >= ncol) break;
+        T acc[PTS][VW];
+#pragma unroll
+        for (int k = 0; k < PTS; ++k)
+#pragma unroll
+            for (int c = 0; c < VW; ++c) acc[k][c] = T(0);
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            V16 av = al_s[so[0] + j * NV + g];
+#pragma unroll
+            for (int k = 0; k < PTS; ++k) {
+                if (k > 0 && so[k] != so[k - 1]) av = al_s[so[k] + j * NV + g];
+                const T* v = reinterpret_cast<const T*>(&av);
+                if constexpr (kF32) {
+                    const float2 x = make_float2(cj[j][k], cj[j][k]);
+#pragma unroll
+                    for (int c = 0; c < VW; c += 2) {
+                        const float2 r = __ffma2_rn(x, make_float2(v[c], v[c + 1]), make_float2(acc[k][c], acc[k][c + 1]));
+                        acc[k][c] = r.x;
+                        acc[k][c + 1] = r.y;
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < VW; ++c) acc[k][c] = fma(cj[j][k], v[c], acc[k][c]);
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < VW; ++c) {
+            if (col + c >= ncol) break;
+            T* dst = W + (long long)(col + c) * ldw + m0;
+            if (npt == PTS) {
+                V16 o;
+                T* op = reinterpret_cast<T*>(&o);
+#pragma unroll
+                for (int k = 0; k < PTS; ++k) op[k] = acc[k][c];
+                *reinterpret_cast<V16*>(dst) = o;
+            } else {
+#pragma unroll
+                for (int k = 0; k < PTS; ++k)
+                    if (k < npt) dst[k] = acc[k][c];
+            }
+        }
+    }
+}
+
 // Nonlocal force reduction for one direction (src/physics/Forces.cpp:772-777, :682-684):
 //   force[a * 3 + dim] = -spn * sum_n occ[n] sum_{j < np(a)} Gamma[poff+j] Re(conj(alpha) beta)
 // and, for dim == 0, the atom's energy share  ea[a] = efac * sum_n occ[n] sum_j Gamma |alpha|^2.

@@ -151,7 +151,21 @@ int launch_nl_expand(const NLDev& nl, T* W, long long ldw, int ncol, const T* al
         const int NP = nl.max_np <= 4 ? 4 : nl.max_np <= 9 ? 9 : nl.max_np <= 18 ? 18 : 32;
         const size_t nrow = (size_t)nl.exp_amax * NP;
         const size_t smem = (size_t)NP * kExpTilePts * sizeof(T) + 2 * nrow * 16;
-        if (nl.exp_tile_atoms && nrow <= 1024 && smem <= 200 * 1024 && (ldw % 4) == 0) {
+        const size_t smem_reg = (size_t)nl.exp_amax * (NP * kExpRegCols * sizeof(T) + 16);
+        if (NP <= 18 && nl.exp_tile_atoms && smem_reg <= 96 * 1024 && (ldw % 4) == 0) {
+            // projector values in registers (up to 18 per point), alpha staged in shared memory
+            dim3 grid((nl.n_pts + kExpTilePts - 1) / kExpTilePts, (ncol + kExpRegCols - 1) / kExpRegCols);
+            auto go = [&](auto kern) -> int {
+                LYNX_CUDA_TRY(smem_cap(kern, smem_reg));
+                kern<<<grid, exp_reg_threads<T>(), smem_reg, st>>>(W, ldw, ncol, ncolp, nl.n_pts, nl.max_np, chi_pt,
+                                                             nl.pt_slot, nl.exp_tile_atoms, nl.exp_amax, nl.atom_poff,
+                                                             nl.atom_nproj, alpha);
+                return LYNX_OK;
+            };
+            if (NP == 4) LYNX_TRY(go(nl_expand_reg_kernel<T, 4>));
+            else if (NP == 9) LYNX_TRY(go(nl_expand_reg_kernel<T, 9>));
+            else LYNX_TRY(go(nl_expand_reg_kernel<T, 18>));
+        } else if (nl.exp_tile_atoms && nrow <= 1024 && smem <= 200 * 1024 && (ldw % 4) == 0) {
             dim3 grid((nl.n_pts + kExpTilePts - 1) / kExpTilePts, (ncol + CBN - 1) / CBN);
             auto go = [&](auto kern) -> int {
                 LYNX_CUDA_TRY(smem_cap(kern, smem));

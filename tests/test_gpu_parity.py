@@ -246,26 +246,28 @@ def test_mixed_pass_tensor_core_gram(system, nstates):
 
 
 def test_fused_nonlocal_and_shapes_bitwise(system):
-    """The fused nonlocal term (stencil kernel adds a * chi alpha) and every launch shape give
-    bitwise the results of the separate-scatter default-shape path (same operations, same order)."""
+    """The fused nonlocal term (stencil kernel adds a * chi alpha), with the projections read from
+    the full grid or from the compact sphere-point copy the previous step wrote, and every launch
+    shape give bitwise the results of the separate-scatter default-shape path (same operations,
+    same order)."""
     from lynx_b200 import _lib
     s = system
     lo, hi, lc = _bounds(s)
     X = C.random_orbitals(s["ctx"].nd, 20, seed=91)
     out = {}
-    for fuse in (0, 1):
-        for tune in (0, 1):
-            ctx = s["solver"].Context(s["cell"])
-            ctx.set_nonlocal(P.nonlocal_tables(s["cell"], s["pos"], P.read_psp8(s["synth_psp8"])))
-            _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_FUSE_NONLOCAL, fuse))
-            _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_AUTOTUNE, tune))
-            es = s["solver"].EigenSolver(ctx)
-            for prec in ("fp64", "mixed"):
-                out[(fuse, tune, prec)] = es.chebyshev_filter(X, s["V"], lc, lo, hi, 6, precision=prec)
-            ctx.close()
+    for fuse, tune, compact in ((0, 0, 0), (0, 1, 0), (1, 0, 0), (1, 1, 0), (1, 1, 1)):
+        ctx = s["solver"].Context(s["cell"])
+        ctx.set_nonlocal(P.nonlocal_tables(s["cell"], s["pos"], P.read_psp8(s["synth_psp8"])))
+        _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_FUSE_NONLOCAL, fuse))
+        _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_AUTOTUNE, tune))
+        _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_COMPACT_GATHER, compact))
+        es = s["solver"].EigenSolver(ctx)
+        for prec in ("fp64", "mixed"):
+            out[(fuse, tune, compact, prec)] = es.chebyshev_filter(X, s["V"], lc, lo, hi, 6, precision=prec)
+        ctx.close()
     for prec in ("fp64", "mixed"):
-        ref_ = out[(0, 0, prec)]
-        for key in ((0, 1), (1, 0), (1, 1)):
+        ref_ = out[(0, 0, 0, prec)]
+        for key in ((0, 1, 0), (1, 0, 0), (1, 1, 0), (1, 1, 1)):
             assert np.array_equal(out[key + (prec,)], ref_), (key, prec)
 
 
