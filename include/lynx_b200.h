@@ -284,6 +284,38 @@ LYNX_API int lynx_eigensolver_solve_density(lynx_ctx* ctx, double* psi, double* 
                                             int precision, double* lambda_cutoff_out, double nelectron, double beta,
                                             int smearing, double weight, double* rho, double* ef_out);
 
+/* ---- Effective potential (the V_eff build of an SCF iteration), FP64, device pointers to fields
+ * of Nd points (x fastest), spin-unpolarised. ---- */
+
+/* GGA-PBE exchange-correlation: exc (energy per particle), vxc = d(rho eps)/d rho - div(2
+ * d(rho eps)/d sigma lapc_T grad rho), and, when dxcdgrho is not NULL, 2 d(rho eps)/d sigma.  The
+ * functional sees rho, or max(rho + rho_core, 1e-14) when rho_core is not NULL; points with a
+ * density <= 1e-14 contribute nothing.  Gradients are the FD first derivatives of the context's
+ * order with its boundary conditions.  Replaces XCFunctional::evaluate for XCType::GGA_PBE
+ * (src/xc/XCFunctional.hpp:41; src/xc/XCFunctional.cpp:193-273), which calls libxc's
+ * XC_GGA_X_PBE + XC_GGA_C_PBE; this library evaluates its own restatement of the published
+ * functional (PBE 1996 with PW92 correlation). */
+LYNX_API int lynx_xc_gga_pbe(lynx_ctx* ctx, const double* rho, const double* rho_core, double* vxc, double* exc,
+                             double* dxcdgrho);
+
+/* Poisson equation -Lap phi = rhs by AAR (m = 7 history columns, Anderson every 6th step,
+ * omega = beta = 0.6, Jacobi preconditioner), phi the start on entry and the solution on return;
+ * stops when ||rhs + Lap phi|| <= tol ||rhs|| (checked after Anderson steps) or after max_iter
+ * steps (<= 0: 3000).  *iters (may be NULL) receives the step count.  rhs is used as given: for a
+ * periodic cell it must have zero mean.  Replaces PoissonSolver::solve
+ * (src/solvers/PoissonSolver.hpp:58; src/solvers/PoissonSolver.cpp:43-159). */
+LYNX_API int lynx_poisson_solve(lynx_ctx* ctx, const double* rhs, double* phi, double tol, int max_iter, int* iters);
+
+/* V_eff = V_xc + phi: GGA-PBE as lynx_xc_gga_pbe (rho_core may be NULL), then phi from
+ * -Lap phi = 4 pi rho + 4 pi rho_b (rho_b, the pseudocharge, may be NULL) with the right-hand
+ * side's mean removed, phi (start on entry) shifted to zero mean.  veff, vxc, exc, phi: Nd
+ * doubles each; *poisson_iters may be NULL.  Replaces EffectivePotential::compute for one spin
+ * channel without NLCC spinors or mGGA (src/physics/EffectivePotential.hpp:58-66;
+ * src/physics/EffectivePotential.cpp:44-177). */
+LYNX_API int lynx_effective_potential(lynx_ctx* ctx, const double* rho, const double* rho_b, const double* rho_core,
+                                      double poisson_tol, double* veff, double* vxc, double* exc, double* phi,
+                                      int* poisson_iters);
+
 /* Diagnostic, no counterpart in the reference: one CTA waits, with at most `spins` tries
  * (1 .. 2^20), for an mbarrier phase that nothing completes, with the same bounded wait the
  * pipelined kernels use for their copies.  The wait gives up and the kernel returns; the call

@@ -92,6 +92,9 @@ _SIGNATURES = {
     "lynx_eigensolver_solve_density": (_c_int, [_p, _p, _pd, _p, _c_int, _c_int, _c_double, _c_double, _c_double,
                                                 _c_int, _c_int, _pd, _c_double, _c_double, _c_int, _c_double, _p,
                                                 _pd]),
+    "lynx_xc_gga_pbe": (_c_int, [_p, _p, _p, _p, _p, _p]),
+    "lynx_poisson_solve": (_c_int, [_p, _p, _p, _c_double, _c_int, _pi]),
+    "lynx_effective_potential": (_c_int, [_p, _p, _p, _p, _c_double, _p, _p, _p, _p, _pi]),
 }
 
 EXPORTED = tuple(_SIGNATURES)

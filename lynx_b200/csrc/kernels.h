@@ -6,6 +6,8 @@
 
 namespace lynxb {
 
+constexpr int kMaxR1 = 9;  // FD half-width bound + 1 (coefficient arrays 0..R)
+
 // Geometry + FD coefficients of one cell for the fused stencil kernel.
 struct StencilGeom {
     int nx, ny, nz;
@@ -127,6 +129,46 @@ int launch_rot_i8(const float* Y, long long ldy, long long rows, int nx, int nxp
 template <typename T>
 int launch_density(const T* psi, long long ld, long long nd, int ncol, const double* w, double* rho, bool accumulate,
                    cudaStream_t st);
+
+// Effective potential (veff.cu), FP64 fields of nx ny nz points, x fastest.
+struct GradGeom {
+    int nx, ny, nz, R;
+    int periodic[3];          // per direction: 1 periodic ghosts, 0 zero (Dirichlet) ghosts
+    double D1[3][kMaxR1];     // first-derivative weights / spacing, index 1..R
+};
+struct XcMetric {
+    int orth;
+    double L[9];  // lapc_T, row-major (non-orthogonal cells)
+};
+constexpr int kAarMaxHist = 16;
+struct AarGamma {
+    int cols;
+    double g[kAarMaxHist];
+};
+constexpr int kMaxDots = 48;
+struct DotList {
+    int count;
+    const double* u[kMaxDots];
+    const double* v[kMaxDots];
+};
+int launch_grad3(const double* x, const GradGeom& g, double* dx, double* dy, double* dz, cudaStream_t st);
+int launch_div_sub(double* v, const GradGeom& g, const double* fx, const double* fy, const double* fz,
+                   cudaStream_t st);
+int launch_rho_xc(const double* rho, const double* core, double* out, long long nd, cudaStream_t st);
+// GGA-PBE per point; on return gx, gy, gz hold the GGA flux v2xc lapc_T grad(rho).
+int launch_pbe(const double* rho, long long nd, const XcMetric& m, double* gx, double* gy, double* gz, double* vxc,
+               double* exc, double* v2xc, cudaStream_t st);
+int launch_aar_pre(const double* r, const double* x, double* x_old, double* f, double* f_old, double* X, double* F,
+                   double w, long long n, cudaStream_t st);
+int launch_aar_update(double* x, const double* x_old, const double* f, const double* X, const double* F,
+                      const AarGamma& g, double c, long long n, cudaStream_t st);
+int launch_sub(const double* b, const double* a, double* r, long long n, cudaStream_t st);
+// out = sa a (+ sa b) - s  (b may be null)
+int launch_add_shift(const double* a, const double* b, double s, double sa, double* out, long long n,
+                     cudaStream_t st);
+size_t dots_work_bytes();
+// Dot products u_k . v_k (deterministic order), copied to host_out; synchronises the stream.
+int launch_dots(const DotList& L, long long n, void* work, double* host_out, cudaStream_t st);
 
 // Launches issued by the library (diagnostic counter, incremented by every launcher).
 void count_launch(int n = 1);

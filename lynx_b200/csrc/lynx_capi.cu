@@ -286,6 +286,8 @@ struct lynx_ctx {
         double* rho = nullptr;
     } dens;
     DevBuf dens_w, dens_part;
+    // effective potential: AAR / XC work fields, a zero potential and a ones field, dot-product scratch
+    DevBuf vwork, vzero, vones, dotw, xcwork;
     // lynx_time_filter_step with with_nonlocal = 2: events around the stencil kernel alone
     bool time_stencil = false;
     cudaEvent_t kt[2] = {nullptr, nullptr};
@@ -2486,6 +2488,234 @@ extern "C" int lynx_eigensolver_solve_density(lynx_ctx* c, double* psi, double* 
         LYNX_TRY(lynx_electron_density(c, psi, nband, ld, occ.data(), weight, rho, 0, 0));
     }
     if (ef_out) *ef_out = c->dens.ef;
+    return LYNX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Effective potential (src/physics/EffectivePotential.cpp:44-177): GGA-PBE exchange-correlation,
+// the AAR Poisson solve and V_eff = V_xc + phi, FP64 on one field of Nd points.
+// ---------------------------------------------------------------------------
+namespace {
+
+GradGeom grad_geom(const lynx_ctx* c) {
+    GradGeom g{};
+    g.nx = c->nx;
+    g.ny = c->ny;
+    g.nz = c->nz;
+    g.R = c->R;
+    for (int d = 0; d < 3; ++d) g.periodic[d] = c->bc[d] == LYNX_BC_PERIODIC ? 1 : 0;
+    for (int p = 0; p <= c->R; ++p) {
+        g.D1[0][p] = c->D1x[p];
+        g.D1[1][p] = c->D1y[p];
+        g.D1[2][p] = c->D1z[p];
+    }
+    return g;
+}
+
+// -Lap x on one field, the Poisson operator (src/solvers/PoissonSolver.cpp:248-253, a = -1): the
+// Chebyshev step kernel with V = 0, a = 2 (a * (-1/2) Lap), b = d = 0 and the nonlocal term off.
+int neg_laplacian(lynx_ctx* c, const double* x, double* out) {
+    LYNX_TRY(ensure_zeroed(c, c->vzero, sizeof(double) * (size_t)c->Nd));
+    const bool nl = c->has_nl;
+    c->has_nl = false;
+    const int st = cheb_step<double>(c, c->nx, x, c->Nd, nullptr, 0, out, c->Nd, c->vzero.as<double>(), 1, 2.0, 0.0,
+                                     0.0, false);
+    c->has_nl = nl;
+    return st;
+}
+
+// Gaussian elimination with partial pivoting on a small dense system, rows whose pivot is below
+// 1e-14 in magnitude skipped in both sweeps: the rule of src/core/NumericalMethods.cpp:84-113,
+// which the AAR step relies on when its history columns are nearly dependent.  A: n x n row-major
+// (overwritten), b: right-hand side, overwritten by the solution.
+void solve_small(std::vector<double>& A, std::vector<double>& b, int n) {
+    for (int k = 0; k < n; ++k) {
+        int piv = k;
+        for (int i = k + 1; i < n; ++i)
+            if (std::fabs(A[i * n + k]) > std::fabs(A[piv * n + k])) piv = i;
+        if (piv != k) {
+            for (int j = 0; j < n; ++j) std::swap(A[k * n + j], A[piv * n + j]);
+            std::swap(b[k], b[piv]);
+        }
+        const double d = A[k * n + k];
+        if (std::fabs(d) < 1e-14) continue;
+        for (int i = k + 1; i < n; ++i) {
+            const double f = A[i * n + k] / d;
+            for (int j = k + 1; j < n; ++j) A[i * n + j] -= f * A[k * n + j];
+            b[i] -= f * b[k];
+        }
+    }
+    for (int k = n - 1; k >= 0; --k) {
+        if (std::fabs(A[k * n + k]) < 1e-14) continue;
+        for (int j = k + 1; j < n; ++j) b[k] -= A[k * n + j] * b[j];
+        b[k] /= A[k * n + k];
+    }
+}
+
+int dots(lynx_ctx* c, const DotList& L, double* out) {
+    LYNX_TRY(c->dotw.ensure(dots_work_bytes()));
+    return launch_dots(L, c->Nd, c->dotw.p, out, c->stream);
+}
+
+// AAR iteration for -Lap phi = b (src/solvers/PoissonSolver.cpp:43-159, CPU semantics: b is
+// used as given, phi is the start and the result).  m history columns, Anderson every p-th
+// step, Richardson weight omega, Anderson weight beta, Jacobi weight -1 / (D2x[0] + D2y[0] +
+// D2z[0]) (:17-37); stops when ||b - A phi|| <= tol ||b||, checked after Anderson steps only.
+int poisson_aar(lynx_ctx* c, const double* b, double* phi, double tol, int max_iter, int* iters) {
+    const int m = 7, p = 6;
+    const double omega = 0.6, beta = 0.6;
+    const long long N = c->Nd;
+    const double diag = c->D2x[0] + c->D2y[0] + c->D2z[0];
+    const double w = std::fabs(diag) < 1e-14 ? 1.0 : -1.0 / diag;
+    LYNX_TRY(c->vwork.ensure(sizeof(double) * (size_t)N * (5 + 2 * m)));
+    double* base = c->vwork.as<double>();
+    double* r = base;
+    double* f = base + N;
+    double* f_old = base + 2 * N;
+    double* x_old = base + 3 * N;
+    double* Ax = base + 4 * N;
+    double* X = base + 5 * N;
+    double* F = X + (size_t)m * N;
+    LYNX_CUDA_TRY(cudaMemsetAsync(f_old, 0, sizeof(double) * N, c->stream));
+    LYNX_CUDA_TRY(cudaMemcpyAsync(x_old, phi, sizeof(double) * N, cudaMemcpyDeviceToDevice, c->stream));
+    DotList L{};
+    L.count = 1;
+    L.u[0] = b;
+    L.v[0] = b;
+    double bn2 = 0.0;
+    LYNX_TRY(dots(c, L, &bn2));
+    const double abs_tol = tol * std::sqrt(bn2);
+    LYNX_TRY(neg_laplacian(c, phi, Ax));
+    LYNX_TRY(launch_sub(b, Ax, r, N, c->stream));
+    double rn = abs_tol + 1.0;
+    int it = 0;
+    while (rn > abs_tol && it < max_iter) {
+        const int col = it > 0 ? (it - 1) % m : -1;
+        LYNX_TRY(launch_aar_pre(r, phi, x_old, f, f_old, col >= 0 ? X + (size_t)col * N : nullptr,
+                                col >= 0 ? F + (size_t)col * N : nullptr, w, N, c->stream));
+        AarGamma g{};
+        if ((it + 1) % p == 0 && it > 0) {
+            const int cols = std::min(it, m);
+            DotList D{};
+            int k = 0;
+            for (int i = 0; i < cols; ++i) {
+                D.u[k] = F + (size_t)i * N;
+                D.v[k++] = f;
+            }
+            for (int i = 0; i < cols; ++i)
+                for (int j = 0; j <= i; ++j) {
+                    D.u[k] = F + (size_t)i * N;
+                    D.v[k++] = F + (size_t)j * N;
+                }
+            D.count = k;
+            double vals[kMaxDots];
+            LYNX_TRY(dots(c, D, vals));
+            std::vector<double> A((size_t)cols * cols), gam(vals, vals + cols);
+            for (int i = 0, q = cols; i < cols; ++i)
+                for (int j = 0; j <= i; ++j, ++q) A[i * cols + j] = A[j * cols + i] = vals[q];
+            solve_small(A, gam, cols);
+            g.cols = cols;
+            for (int i = 0; i < cols; ++i) g.g[i] = gam[i];
+            LYNX_TRY(launch_aar_update(phi, x_old, f, X, F, g, beta, N, c->stream));
+            LYNX_TRY(neg_laplacian(c, phi, Ax));
+            LYNX_TRY(launch_sub(b, Ax, r, N, c->stream));
+            DotList R{};
+            R.count = 1;
+            R.u[0] = r;
+            R.v[0] = r;
+            double rr = 0.0;
+            LYNX_TRY(dots(c, R, &rr));
+            rn = std::sqrt(rr);
+        } else {
+            g.cols = 0;
+            LYNX_TRY(launch_aar_update(phi, x_old, f, X, F, g, omega, N, c->stream));
+            LYNX_TRY(neg_laplacian(c, phi, Ax));
+            LYNX_TRY(launch_sub(b, Ax, r, N, c->stream));
+        }
+        ++it;
+    }
+    if (iters) *iters = it;
+    LYNX_TRY(check_errflag(c));
+    return LYNX_OK;
+}
+
+// Sum of a field (the global mean over Nd points is sum / Nd).
+int field_sum(lynx_ctx* c, const double* x, double* sum) {
+    if (c->vones.bytes < sizeof(double) * (size_t)c->Nd) {
+        LYNX_TRY(ensure_zeroed(c, c->vzero, sizeof(double) * (size_t)c->Nd));
+        LYNX_TRY(c->vones.ensure(sizeof(double) * (size_t)c->Nd));
+        LYNX_TRY(launch_add_shift(c->vzero.as<double>(), nullptr, -1.0, 1.0, c->vones.as<double>(), c->Nd, c->stream));
+    }
+    DotList L{};
+    L.count = 1;
+    L.u[0] = x;
+    L.v[0] = c->vones.as<double>();
+    return dots(c, L, sum);
+}
+
+}  // namespace
+
+extern "C" int lynx_xc_gga_pbe(lynx_ctx* c, const double* rho, const double* rho_core, double* vxc, double* exc,
+                               double* dxcdgrho) {
+    LYNX_CHECK_ARG(c && rho && vxc && exc, "null pointer");
+    LYNX_CHECK_ARG(c->nx > c->R && c->ny > c->R && c->nz > c->R, "grid smaller than the FD half-width");
+    LYNX_TRY(activate(c));
+    const long long N = c->Nd;
+    // scratch: 3 gradient / flux fields and the core-corrected density
+    LYNX_TRY(c->xcwork.ensure(sizeof(double) * (size_t)N * 4));
+    double* gx = c->xcwork.as<double>();
+    double* gy = gx + N;
+    double* gz = gy + N;
+    const double* rx = rho;
+    if (rho_core) {
+        double* t = gz + N;
+        LYNX_TRY(launch_rho_xc(rho, rho_core, t, N, c->stream));
+        rx = t;
+    }
+    const GradGeom g = grad_geom(c);
+    LYNX_TRY(launch_grad3(rx, g, gx, gy, gz, c->stream));
+    XcMetric mt{};
+    mt.orth = c->orth ? 1 : 0;
+    for (int i = 0; i < 9; ++i) mt.L[i] = c->lapcT[i];
+    LYNX_TRY(launch_pbe(rx, N, mt, gx, gy, gz, vxc, exc, dxcdgrho, c->stream));
+    LYNX_TRY(launch_div_sub(vxc, g, gx, gy, gz, c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return LYNX_OK;
+}
+
+extern "C" int lynx_poisson_solve(lynx_ctx* c, const double* rhs, double* phi, double tol, int max_iter, int* iters) {
+    LYNX_CHECK_ARG(c && rhs && phi, "null pointer");
+    LYNX_CHECK_ARG(tol > 0.0, "tol must be positive");
+    LYNX_CHECK_ARG(c->nx > c->R && c->ny > c->R && c->nz > c->R, "grid smaller than the FD half-width");
+    LYNX_TRY(activate(c));
+    LYNX_TRY(poisson_aar(c, rhs, phi, tol, max_iter > 0 ? max_iter : 3000, iters));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return LYNX_OK;
+}
+
+extern "C" int lynx_effective_potential(lynx_ctx* c, const double* rho, const double* rho_b, const double* rho_core,
+                                        double poisson_tol, double* veff, double* vxc, double* exc, double* phi,
+                                        int* poisson_iters) {
+    LYNX_CHECK_ARG(c && rho && veff && vxc && exc && phi, "null pointer");
+    LYNX_CHECK_ARG(poisson_tol > 0.0, "poisson_tol must be positive");
+    LYNX_TRY(activate(c));
+    const long long N = c->Nd;
+    // 1. exchange-correlation
+    LYNX_TRY(lynx_xc_gga_pbe(c, rho, rho_core, vxc, exc, nullptr));
+    // 2. Poisson: rhs = 4 pi rho + 4 pi rho_b with its mean removed;
+    //    the right-hand side is built in veff, which is written last (EffectivePotential.cpp:44-60)
+    const double fpi = 4.0 * 3.14159265358979323846;
+    LYNX_TRY(launch_add_shift(rho, rho_b, 0.0, fpi, veff, N, c->stream));
+    double sum = 0.0;
+    LYNX_TRY(field_sum(c, veff, &sum));
+    LYNX_TRY(launch_add_shift(veff, nullptr, sum / (double)N, 1.0, veff, N, c->stream));
+    LYNX_TRY(poisson_aar(c, veff, phi, poisson_tol, 3000, poisson_iters));
+    // phi shifted to zero mean (EffectivePotential.cpp:64-70)
+    LYNX_TRY(field_sum(c, phi, &sum));
+    LYNX_TRY(launch_add_shift(phi, nullptr, sum / (double)N, 1.0, phi, N, c->stream));
+    // 3. V_eff = V_xc + phi
+    LYNX_TRY(launch_add_shift(vxc, phi, 0.0, 1.0, veff, N, c->stream));
+    LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return LYNX_OK;
 }
 

@@ -55,6 +55,8 @@ _SIG = {
     "ref_nonlocal_force": (_i, [_pd, _pd, _i, _i, _pd, _d, _pd]),
     "ref_kinetic_nonlocal_stress": (_i, [_pd, _pd, _i, _i, _pd, _d, _pd, _pd]),
     "ref_density": (_i, [_pd, _pd, _i, _i, _d, _pd]),
+    "ref_poisson": (_i, [_pd, _pd, _d, _pi]),
+    "ref_gradient": (_i, [_pd, _pd, _i]),
 }
 
 _lib = None
@@ -275,6 +277,22 @@ class RefLynx:
         rho = np.zeros(self.nd)
         _chk(lib().ref_density(x.ctypes.data_as(_pd), _p(o), x.shape[1], int(complex_), float(wk), _p(rho)))
         return rho
+
+    def poisson(self, rhs, phi0=None, tol=1e-8):
+        """PoissonSolver::solve (src/solvers/PoissonSolver.cpp:43-159): -Lap phi = rhs from phi0
+        (zeros); returns (phi, iterations)."""
+        b = np.ascontiguousarray(rhs, dtype=np.float64).ravel()
+        phi = np.zeros(self.nd) if phi0 is None else np.ascontiguousarray(phi0, dtype=np.float64).ravel().copy()
+        it = ctypes.c_int(0)
+        _chk(lib().ref_poisson(_p(b), _p(phi), float(tol), ctypes.byref(it)))
+        return phi, it.value
+
+    def gradient(self, x, dim):
+        """Gradient::apply of one field along direction dim (src/operators/Gradient.cpp:17-62)."""
+        v = np.ascontiguousarray(x, dtype=np.float64).ravel()
+        y = np.zeros(self.nd)
+        _chk(lib().ref_gradient(_p(v), _p(y), int(dim)))
+        return y
 
     def kpoints(self, kgrid, shift=(0.0, 0.0, 0.0)):
         n = int(np.prod(kgrid))

@@ -50,6 +50,8 @@
 #include "electronic/ElectronDensity.hpp"
 #include "electronic/Wavefunction.hpp"
 #include "operators/Gradient.hpp"
+#include "operators/Laplacian.hpp"
+#include "solvers/PoissonSolver.hpp"
 #include "parallel/Parallelization.hpp"
 #include "physics/Forces.hpp"
 #include "physics/Stress.hpp"
@@ -501,6 +503,28 @@ int ref_density(const double* psi, const double* occ, int nband, int is_kpt, dou
 void ref_randomize(double* x, long n, unsigned seed) {
     std::srand(seed);
     for (long i = 0; i < n; ++i) x[i] = -0.5 + 1.0 * ((double)std::rand() / RAND_MAX);
+}
+
+// PoissonSolver::solve on the set-up grid (src/solvers/PoissonSolver.cpp:17-159): -Lap phi = rhs
+// from the start phi; *iters receives the AAR step count.
+int ref_poisson(const double* rhs, double* phi, double tol, int* iters) {
+    return guarded([&] {
+        lynx::Laplacian lap(g->stencil, g->domain);
+        lynx::PoissonSolver ps;
+        ps.setup(lap, g->stencil, g->domain, g->grid, g->halo);
+        *iters = ps.solve(rhs, phi, tol);
+    });
+}
+
+// Gradient::apply along direction dir of one field, ghosts from HaloExchange::execute
+// (src/operators/Gradient.cpp:17-62).
+int ref_gradient(const double* x, double* y, int dir) {
+    return guarded([&] {
+        lynx::Gradient grad(g->stencil, g->domain);
+        std::vector<double> xe(g->halo.nd_ex(), 0.0);
+        g->halo.execute(x, xe.data(), 1);
+        grad.apply(xe.data(), y, dir, 1);
+    });
 }
 
 int ref_set_threads(int n) {
