@@ -135,6 +135,8 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-scf", action="store_true", help="skip the SCF-iteration summary (pass + density + V_eff)")
+    p.add_argument("--no-batch", action="store_true", help="skip the batched k-point + ensemble summary")
     p.add_argument("--profile-pass", action="store_true",
                    help="bracket the first timed pass with cudaProfilerStart/Stop, so that "
                         "`ncu --profile-from-start off` captures exactly one pass")
@@ -417,6 +419,10 @@ def main():
     achieved = fused_bytes / (ms_k.value * 1e-3) / 1e9
     updates = ctx.nd * nst * degree
 
+    scf = None
+    if rank == 0 and not args.no_scf:
+        scf = scf_iteration_summary(ctx, es, psi, Vd, lc, emin, hi, degree, natom)
+
     e2e = None
     if not args.no_e2e:
         host_psi = torch.empty((nst, ctx.nd), dtype=torch.float64, pin_memory=True)
@@ -473,7 +479,10 @@ def main():
             "gpu_launches": launches,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "scf_iteration": scf,
         }
+        if not args.no_batch:
+            line["batch"] = batch_summary()
         print(json.dumps(line))
     ctx.close()
     if world > 1:
@@ -555,76 +564,161 @@ def run_reference_batch(args, rank, world):
         pass
 
 
-def run_batch(args, rank, world, local):
-    """The batched workload: every problem on its own context, one pass over all of them per
-    step through solve_batch (lynx_eigensolver_solve_batch), against the same passes run one
-    after another."""
-    import torch
-    import torch.distributed as dist
-    from lynx_b200 import solver
+class BatchRun:
+    """The batched workload on this process's GPU: every problem on its own context; passes over
+    all of them through solve_batch (lynx_eigensolver_solve_batch), or one after another."""
 
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-    degree = 20
-    probs, psp_path = build_batch()
-    solvers, lo_hi, psis, Vs = [], [], [], []
-    gen = torch.Generator(device="cuda").manual_seed(replica_seed(rank))
-    for pb in probs:
-        ctx = solver.Context(pb.cell, device=local)
-        ctx.set_nonlocal(pb.tables)
-        if pb.complex:
-            ctx.set_kpoint(pb.kcart)
-        es = solver.EigenSolver(ctx, args.precision)
-        V = torch.from_numpy(pb.veff).cuda()
-        lo, hi = es.lanczos_bounds(V, kpt=pb.complex)
-        solvers.append(es)
-        lo_hi.append([0.5 * (lo + hi), lo, hi])
-        Vs.append(V)
-        x = torch.rand((pb.nband, ctx.nd), generator=gen, device="cuda", dtype=torch.float64) - 0.5
-        if pb.complex:
-            y = torch.rand((pb.nband, ctx.nd), generator=gen, device="cuda", dtype=torch.float64) - 0.5
-            x = torch.complex(x, y)
-        psis.append(x.contiguous())
-    kflags = [pb.complex for pb in probs]
+    def __init__(self, rank, degree=20):
+        import torch
+        from lynx_b200 import solver
+        self.solver = solver
+        self.degree = degree
+        self.probs, self.psp_path = build_batch()
+        self.solvers, self.lo_hi, self.psis, self.Vs = [], [], [], []
+        gen = torch.Generator(device="cuda").manual_seed(replica_seed(rank))
+        for pb in self.probs:
+            ctx = solver.Context(pb.cell, device=torch.cuda.current_device())
+            ctx.set_nonlocal(pb.tables)
+            if pb.complex:
+                ctx.set_kpoint(pb.kcart)
+            es = solver.EigenSolver(ctx, "mixed")
+            V = torch.from_numpy(pb.veff).cuda()
+            lo, hi = es.lanczos_bounds(V, kpt=pb.complex)
+            self.solvers.append(es)
+            self.lo_hi.append([0.5 * (lo + hi), lo, hi])
+            self.Vs.append(V)
+            x = torch.rand((pb.nband, ctx.nd), generator=gen, device="cuda", dtype=torch.float64) - 0.5
+            if pb.complex:
+                y = torch.rand((pb.nband, ctx.nd), generator=gen, device="cuda", dtype=torch.float64) - 0.5
+                x = torch.complex(x, y)
+            self.psis.append(x.contiguous())
+        self.kflags = [pb.complex for pb in self.probs]
 
-    def batched(precision, host=None):
-        res = solver.solve_batch(solvers, host if host is not None else psis, Vs, [b[0] for b in lo_hi],
-                                 [b[1] for b in lo_hi], [b[2] for b in lo_hi], degree, precision=precision,
-                                 kpt=kflags)
-        for b, es, (_, eig) in zip(lo_hi, solvers, res):
+    def batched(self, precision, host=None):
+        res = self.solver.solve_batch(self.solvers, host if host is not None else self.psis, self.Vs,
+                                      [b[0] for b in self.lo_hi], [b[1] for b in self.lo_hi], [b[2] for b in self.lo_hi],
+                                      self.degree, precision=precision, kpt=self.kflags)
+        for b, es, (_, eig) in zip(self.lo_hi, self.solvers, res):
             b[0] = es.lambda_cutoff()
             b[1] = float(eig[0])
         return res
 
-    def sequential(precision):
-        for pb, es, b, p, V in zip(probs, solvers, lo_hi, psis, Vs):
+    def sequential(self, precision):
+        for pb, es, b, p, V in zip(self.probs, self.solvers, self.lo_hi, self.psis, self.Vs):
             fn = es.solve_kpt if pb.complex else es.solve
-            _, eig = fn(p, V, b[0], b[1], b[2], degree, precision=precision)
+            _, eig = fn(p, V, b[0], b[1], b[2], self.degree, precision=precision)
             b[0] = es.lambda_cutoff()
             b[1] = float(eig[0])
 
-    def timed(fn, k):
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(k):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / 1e3 / k
+    def close(self):
+        for es in self.solvers:
+            es.ctx.close()
+        try:
+            os.remove(self.psp_path)
+        except OSError:
+            pass
+
+
+def timed_device(fn, k, world=1):
+    """Seconds per call of fn over k calls, CUDA events on torch's current stream."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(k):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / k
+
+
+def batch_summary():
+    """The batched k-point + strained-ensemble workload, measured beside the headline: s per pass
+    over all problems through solve_batch, mixed and FP64, and the mixed passes one after another."""
+    B = BatchRun(0)
+    try:
+        for _ in range(2):
+            B.batched("mixed")
+        B.batched("fp64")
+        B.sequential("mixed")
+        t_mixed = timed_device(lambda: B.batched("mixed"), 3)
+        t_fp64 = timed_device(lambda: B.batched("fp64"), 2)
+        t_seq = timed_device(lambda: B.sequential("mixed"), 2)
+        return {"workload": "batched CheFSI pass: 36 k-points Si2 FCC 20^3 N=16 (complex) + 32 strained Si8 "
+                            "24-32^3 N=24, degree 20", "problems": len(B.probs), "mixed_s_per_pass": t_mixed,
+                "fp64_s_per_pass": t_fp64, "speedup_vs_fp64": t_fp64 / t_mixed,
+                "sequential_mixed_s_per_pass": t_seq, "speedup_vs_sequential": t_seq / t_mixed,
+                "api": "lynx_eigensolver_solve_batch (one host thread and stream per problem)"}
+    finally:
+        B.close()
+
+
+def scf_iteration_summary(ctx, es, psi, Vd, lc, emin, hi, degree, natom, reps=2):
+    """One SCF iteration at fixed V_eff as the device runs it: the CheFSI pass with the Fermi level
+    (Fermi-Dirac, 0.001 Ha), occupations and density of the new orbitals
+    (lynx_eigensolver_solve_density; in the mixed pass the density is accumulated by the
+    tensor-core rotation), then V_eff = V_xc + phi of that density (GGA-PBE; AAR Poisson from the
+    previous phi, tolerance 1e-8).  The new potential is not fed back (no mixing, and the synthetic
+    V_eff has no pseudocharge), so every iteration solves the same eigenproblem.  Mixing is not
+    included."""
+    import torch
+    from lynx_b200 import potential as Pm
+    pot = Pm.EffectivePotential(ctx)
+    nel = 4.0 * natom
+    st = {"lc": lc, "emin": emin}
+    rho = torch.empty(ctx.nd, dtype=torch.float64, device="cuda")
+    iters = []
+
+    def one(prec):
+        _, eig, _, _ = es.solve_density(psi, Vd, st["lc"], st["emin"], hi, degree, nelectron=nel, beta=1000.0,
+                                        rho=rho, precision=prec)
+        st["lc"] = es.lambda_cutoff()
+        st["emin"] = float(eig[0])
+        iters.append(pot.compute(rho, poisson_tol=1e-8).poisson_iters)
+
+    t0 = time.perf_counter()
+    one("mixed")  # the first V_eff build solves Poisson from phi = 0
+    torch.cuda.synchronize()
+    cold = {"s": time.perf_counter() - t0, "poisson_iters": iters[-1]}
+    out = {"note": "CheFSI pass + Fermi level + density + V_eff build (GGA-PBE + AAR Poisson, tol 1e-8, warm "
+                   "start from the previous phi); V_eff not fed back, mixing not included",
+           "first_iteration_cold_poisson": cold}
+    for prec in ("mixed", "fp64"):
+        one(prec)
+        t = timed_device(lambda: one(prec), reps)
+        out[f"{prec}_s_per_iter"] = t
+    out["veff_build_s"] = timed_device(lambda: pot.compute(rho, poisson_tol=1e-8), 2)
+    out["poisson_iters_warm"] = iters[-1]
+    out["speedup_vs_fp64"] = out["fp64_s_per_iter"] / out["mixed_s_per_iter"]
+    return out
+
+
+def run_batch(args, rank, world, local):
+    """The batched workload as the headline: every problem on its own context, one pass over all
+    of them per step through solve_batch (lynx_eigensolver_solve_batch), against the same passes
+    run one after another."""
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    B = BatchRun(rank)
+    probs, psp_path, psis, degree = B.probs, B.psp_path, B.psis, B.degree
+    batched, sequential = B.batched, B.sequential
 
     for _ in range(args.warmup):
         batched(args.precision)
     sequential(args.precision)
-    lib = solvers[0].ctx.lib
-    t_seq = timed(lambda: sequential(args.precision), max(1, min(2, args.steps)))
+    lib = B.solvers[0].ctx.lib
+    t_seq = timed_device(lambda: sequential(args.precision), max(1, min(2, args.steps)), world)
     lib.lynx_launch_count(1)
     with ClockSampler(local) as clk:
-        t_main = timed(lambda: batched(args.precision), args.steps)
+        t_main = timed_device(lambda: batched(args.precision), args.steps, world)
     launches = int(lib.lynx_launch_count(1))
     t_main = max_over_ranks(t_main, world, "cuda")
 
@@ -679,14 +773,9 @@ def run_batch(args, rank, world, local):
             "e2e": e2e,
             "cpu_baseline": cpu,
         }))
-    for es in solvers:
-        es.ctx.close()
+    B.close()
     if world > 1:
         dist.destroy_process_group()
-    try:
-        os.remove(psp_path)
-    except OSError:
-        pass
 
 
 if __name__ == "__main__":

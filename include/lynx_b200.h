@@ -308,7 +308,9 @@ LYNX_API int lynx_poisson_solve(lynx_ctx* ctx, const double* rhs, double* phi, d
 
 /* V_eff = V_xc + phi: GGA-PBE as lynx_xc_gga_pbe (rho_core may be NULL), then phi from
  * -Lap phi = 4 pi rho + 4 pi rho_b (rho_b, the pseudocharge, may be NULL) with the right-hand
- * side's mean removed, phi (start on entry) shifted to zero mean.  veff, vxc, exc, phi: Nd
+ * side's mean removed, phi (start on entry) shifted to zero mean.  For a periodic cell the
+ * equation is solved by FFT (*poisson_iters = 0) unless LYNX_OPT_POISSON_DIRECT is 0; otherwise,
+ * and for Dirichlet directions, by AAR as lynx_poisson_solve.  veff, vxc, exc, phi: Nd
  * doubles each; *poisson_iters may be NULL.  Replaces EffectivePotential::compute for one spin
  * channel without NLCC spinors or mGGA (src/physics/EffectivePotential.hpp:58-66;
  * src/physics/EffectivePotential.cpp:44-177). */
@@ -351,8 +353,18 @@ LYNX_API int lynx_nonlocal_apply_noalloc(lynx_ctx* ctx, const double* psi, doubl
  *                            its output at the sphere points as a compact block, and the next
  *                            step's projections read that block instead of the full grid; 0
  *                            (default) reads the full grid.  Same results, bitwise.
+ *   LYNX_OPT_POISSON_DIRECT: 1 (default) makes lynx_effective_potential solve the Poisson equation
+ *                            of a periodic cell exactly by FFT (the discrete equation the AAR
+ *                            iteration converges to, to rounding); 0 uses the AAR iteration.
+ *                            lynx_poisson_solve is always the AAR iteration.
  */
-enum { LYNX_OPT_AUTOTUNE = 1, LYNX_OPT_FUSE_NONLOCAL = 2, LYNX_OPT_TC_RAYLEIGH_RITZ = 3, LYNX_OPT_COMPACT_GATHER = 4 };
+enum {
+    LYNX_OPT_AUTOTUNE = 1,
+    LYNX_OPT_FUSE_NONLOCAL = 2,
+    LYNX_OPT_TC_RAYLEIGH_RITZ = 3,
+    LYNX_OPT_COMPACT_GATHER = 4,
+    LYNX_OPT_POISSON_DIRECT = 5
+};
 LYNX_API int lynx_set_option(lynx_ctx* ctx, int option, int value);
 
 /* Number of kernel launches this library issued since the last reset (diagnostic counter). */

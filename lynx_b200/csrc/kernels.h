@@ -166,6 +166,10 @@ int launch_sub(const double* b, const double* a, double* r, long long n, cudaStr
 // out = sa a (+ sa b) - s  (b may be null)
 int launch_add_shift(const double* a, const double* b, double s, double sa, double* out, long long n,
                      cudaStream_t st);
+// Periodic Poisson by FFT: z *= s * scale (half-spectrum), s = 1 / Re(FFT of the operator's
+// impulse response) with the mean mode set to zero.
+int launch_spec_scale(double2* z, const double* s, double scale, long long n, cudaStream_t st);
+int launch_inv_symbol(const double2* g, double* s, long long n, cudaStream_t st);
 size_t dots_work_bytes();
 // Dot products u_k . v_k (deterministic order), copied to host_out; synchronises the stream.
 int launch_dots(const DotList& L, long long n, void* work, double* host_out, cudaStream_t st);

@@ -12,6 +12,7 @@
 #include <cublas_v2.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
+#include <cufft.h>
 #include <curand.h>
 
 #include <algorithm>
@@ -288,6 +289,11 @@ struct lynx_ctx {
     DevBuf dens_w, dens_part;
     // effective potential: AAR / XC work fields, a zero potential and a ones field, dot-product scratch
     DevBuf vwork, vzero, vones, dotw, xcwork;
+    // periodic Poisson by FFT: plans and the inverse symbol of -Lap (made on first use)
+    bool poisson_direct = true;
+    bool fft_ready = false;
+    cufftHandle fft_fwd = 0, fft_inv = 0;
+    DevBuf fft_sym, fft_z;
     // lynx_time_filter_step with with_nonlocal = 2: events around the stencil kernel alone
     bool time_stencil = false;
     cudaEvent_t kt[2] = {nullptr, nullptr};
@@ -1523,6 +1529,13 @@ int lynx_destroy(lynx_ctx* c) {
         kv.second.ptmap.release();
         kv.second.rowstart.release();
     }
+    for (DevBuf* b : {&c->dens_w, &c->dens_part, &c->vwork, &c->vzero, &c->vones, &c->dotw, &c->xcwork, &c->fft_sym,
+                      &c->fft_z})
+        b->release();
+    if (c->fft_ready) {
+        cufftDestroy(c->fft_fwd);
+        cufftDestroy(c->fft_inv);
+    }
     if (c->cublas) cublasDestroy(c->cublas);
     if (c->cusolver) cusolverDnDestroy(c->cusolver);
     delete c;
@@ -2385,6 +2398,7 @@ extern "C" int lynx_set_option(lynx_ctx* c, int option, int value) {
         case LYNX_OPT_FUSE_NONLOCAL: c->fuse_nl = value != 0; return LYNX_OK;
         case LYNX_OPT_TC_RAYLEIGH_RITZ: c->no_tc_gram = value == 0; return LYNX_OK;
         case LYNX_OPT_COMPACT_GATHER: c->fuse_compact_gather = value != 0; return LYNX_OK;
+        case LYNX_OPT_POISSON_DIRECT: c->poisson_direct = value != 0; return LYNX_OK;
         default: set_error("unknown option %d", option); return LYNX_ERR_BAD_ARG;
     }
 }
@@ -2639,6 +2653,51 @@ int poisson_aar(lynx_ctx* c, const double* b, double* phi, double tol, int max_i
     return LYNX_OK;
 }
 
+// Periodic cells: -Lap phi = b solved exactly in Fourier space.  The FD operator (with the
+// mixed-derivative terms of a non-orthogonal cell) is a circular convolution with its own impulse
+// response g = A delta_0, so phi_hat = b_hat / g_hat, the mean mode set to zero.  g comes from the
+// same stencil kernel the AAR iteration applies, so phi solves the same discrete equation, to
+// rounding, instead of to the iteration's tolerance; b must have zero mean.
+int poisson_direct(lynx_ctx* c, const double* b, double* phi) {
+    const long long N = c->Nd;
+    const long long nh = (long long)c->nz * c->ny * (c->nx / 2 + 1);
+    auto fft_check = [](cufftResult r, const char* what) -> int {
+        if (r == CUFFT_SUCCESS) return LYNX_OK;
+        set_error("%s failed (cuFFT status %d)", what, (int)r);
+        return r == CUFFT_ALLOC_FAILED ? LYNX_ERR_OOM : LYNX_ERR_CUDA;
+    };
+    LYNX_TRY(c->fft_z.ensure(sizeof(double2) * (size_t)nh));
+    double2* z = c->fft_z.as<double2>();
+    if (!c->fft_ready) {
+        LYNX_TRY(fft_check(cufftPlan3d(&c->fft_fwd, c->nz, c->ny, c->nx, CUFFT_D2Z), "cufftPlan3d"));
+        if (cufftPlan3d(&c->fft_inv, c->nz, c->ny, c->nx, CUFFT_Z2D) != CUFFT_SUCCESS) {
+            cufftDestroy(c->fft_fwd);
+            set_error("cufftPlan3d (inverse) failed");
+            return LYNX_ERR_CUDA;
+        }
+        c->fft_ready = true;
+        LYNX_TRY(c->fft_sym.ensure(sizeof(double) * (size_t)nh));
+        LYNX_TRY(c->vwork.ensure(sizeof(double) * (size_t)N * 2));
+        double* d = c->vwork.as<double>();
+        double* g = d + N;
+        const double one = 1.0;
+        LYNX_CUDA_TRY(cudaMemsetAsync(d, 0, sizeof(double) * N, c->stream));
+        LYNX_CUDA_TRY(cudaMemcpyAsync(d, &one, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        LYNX_TRY(neg_laplacian(c, d, g));
+        LYNX_TRY(fft_check(cufftSetStream(c->fft_fwd, c->stream), "cufftSetStream"));
+        LYNX_TRY(fft_check(cufftExecD2Z(c->fft_fwd, g, z), "cufftExecD2Z"));
+        LYNX_TRY(launch_inv_symbol(z, c->fft_sym.as<double>(), nh, c->stream));
+        LYNX_CUDA_TRY(cudaStreamSynchronize(c->stream));  // `one` is a host temporary
+    }
+    LYNX_TRY(fft_check(cufftSetStream(c->fft_fwd, c->stream), "cufftSetStream"));
+    LYNX_TRY(fft_check(cufftSetStream(c->fft_inv, c->stream), "cufftSetStream"));
+    LYNX_TRY(fft_check(cufftExecD2Z(c->fft_fwd, const_cast<double*>(b), z), "cufftExecD2Z"));
+    LYNX_TRY(launch_spec_scale(z, c->fft_sym.as<double>(), 1.0 / (double)N, nh, c->stream));
+    LYNX_TRY(fft_check(cufftExecZ2D(c->fft_inv, z, phi), "cufftExecZ2D"));
+    count_launch(3);
+    return LYNX_OK;
+}
+
 // Sum of a field (the global mean over Nd points is sum / Nd).
 int field_sum(lynx_ctx* c, const double* x, double* sum) {
     if (c->vones.bytes < sizeof(double) * (size_t)c->Nd) {
@@ -2709,7 +2768,13 @@ extern "C" int lynx_effective_potential(lynx_ctx* c, const double* rho, const do
     double sum = 0.0;
     LYNX_TRY(field_sum(c, veff, &sum));
     LYNX_TRY(launch_add_shift(veff, nullptr, sum / (double)N, 1.0, veff, N, c->stream));
-    LYNX_TRY(poisson_aar(c, veff, phi, poisson_tol, 3000, poisson_iters));
+    const bool periodic = c->bc[0] == LYNX_BC_PERIODIC && c->bc[1] == LYNX_BC_PERIODIC && c->bc[2] == LYNX_BC_PERIODIC;
+    if (c->poisson_direct && periodic) {
+        LYNX_TRY(poisson_direct(c, veff, phi));
+        if (poisson_iters) *poisson_iters = 0;
+    } else {
+        LYNX_TRY(poisson_aar(c, veff, phi, poisson_tol, 3000, poisson_iters));
+    }
     // phi shifted to zero mean (EffectivePotential.cpp:64-70)
     LYNX_TRY(field_sum(c, phi, &sum));
     LYNX_TRY(launch_add_shift(phi, nullptr, sum / (double)N, 1.0, phi, N, c->stream));

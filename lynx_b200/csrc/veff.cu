@@ -308,6 +308,22 @@ __global__ void add_shift_kernel(const double* __restrict__ a, const double* __r
     }
 }
 
+// z[i] *= s[i] * scale over the half-spectrum of a real 3-D FFT (the periodic Poisson solve).
+__global__ void spec_scale_kernel(double2* __restrict__ z, const double* __restrict__ s, double scale, long long n) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const double f = s[t] * scale;
+        z[t] = make_double2(z[t].x * f, z[t].y * f);
+    }
+}
+
+// s[i] = 1 / Re(g_hat[i]) (0 for the mean mode i = 0 and for modes whose symbol vanishes).
+__global__ void inv_symbol_kernel(const double2* __restrict__ g, double* __restrict__ s, long long n) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const double v = g[t].x;
+        s[t] = (t == 0 || fabs(v) < 1e-300) ? 0.0 : 1.0 / v;
+    }
+}
+
 int grid_for(long long n) {
     long long b = (n + kVThreads - 1) / kVThreads;
     if (b > 148 * 16) b = 148 * 16;
@@ -371,6 +387,16 @@ int launch_add_shift(const double* a, const double* b, double s, double sa, doub
                      cudaStream_t st) {
     add_shift_kernel<<<grid_for(n), kVThreads, 0, st>>>(a, b, s, sa, out, n);
     return launch_ok("shift");
+}
+
+int launch_spec_scale(double2* z, const double* s, double scale, long long n, cudaStream_t st) {
+    spec_scale_kernel<<<grid_for(n), kVThreads, 0, st>>>(z, s, scale, n);
+    return launch_ok("spectral scale");
+}
+
+int launch_inv_symbol(const double2* g, double* s, long long n, cudaStream_t st) {
+    inv_symbol_kernel<<<grid_for(n), kVThreads, 0, st>>>(g, s, n);
+    return launch_ok("Poisson symbol");
 }
 
 size_t dots_work_bytes() { return sizeof(double) * ((size_t)kMaxDots * kDotBlocks + kMaxDots); }

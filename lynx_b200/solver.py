@@ -328,6 +328,31 @@ class EigenSolver:
                   precision: Optional[str] = None):
         return self._solve(psi, Veff, lambda_cutoff, eigval_min, eigval_max, cheb_degree, precision, True)
 
+    def solve_density(self, psi, Veff, lambda_cutoff, eigval_min, eigval_max, cheb_degree: int = 20,
+                      nelectron: float = 0.0, beta: float = 1000.0, smearing: str = "fermi-dirac",
+                      weight: float = 2.0, rho=None, precision: Optional[str] = None):
+        """One CheFSI pass, then the Fermi level, occupations and electron density of the new
+        orbitals (lynx_eigensolver_solve_density; real orbitals, one spin channel and k-point).
+        rho: a device tensor of Nd doubles to write, or None for a new one.  Returns
+        (psi_out, eig, rho, ef)."""
+        ctx = self.ctx
+        torch = _torch()
+        prec = _PREC[precision or self.precision]
+        ctx.sync_stream()
+        a = _DeviceArgs(ctx, psi, False)
+        v = _veff_dev(ctx, Veff)
+        if rho is None:
+            rho = torch.empty(ctx.nd, dtype=torch.float64, device=f"cuda:{ctx.device}")
+        eig = np.zeros(a.ncol)
+        lc_out, ef = ctypes.c_double(), ctypes.c_double()
+        sm = _SMEAR[smearing]
+        check(ctx.lib.lynx_eigensolver_solve_density(
+            ctx.handle, ctypes.c_void_p(_dev_ptr(a.t)), dptr(eig), ctypes.c_void_p(v.data_ptr()), a.ncol, ctx.nd,
+            float(lambda_cutoff), float(eigval_min), float(eigval_max), int(cheb_degree), prec, ctypes.byref(lc_out),
+            float(nelectron), float(beta), sm, float(weight), ctypes.c_void_p(_dev_ptr(rho)), ctypes.byref(ef)))
+        self._lambda_cutoff = lc_out.value
+        return a.out(a.t), eig, rho, ef.value
+
     def chebyshev_filter(self, X, Veff, lambda_cutoff, eigval_min, eigval_max, degree: int = 20,
                          precision: Optional[str] = None, kpt: bool = False):
         ctx = self.ctx

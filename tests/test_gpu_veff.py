@@ -87,21 +87,49 @@ def test_poisson_matches_reference(kind):
     ctx.close()
 
 
-def test_effective_potential_matches_oracle():
+@pytest.mark.parametrize("direct", [1, 0])
+def test_effective_potential_matches_oracle(direct):
+    """V_eff = V_xc + phi against the numpy composition; the periodic Poisson equation solved by
+    FFT (default) or by the AAR iteration."""
+    from lynx_b200 import _lib
     from lynx_b200 import potential as P
     ctx, cl, H, rho = _setup("periodic")
+    ctx.set_option(_lib.OPT_POISSON_DIRECT, direct)
     rho_b = -np.roll(rho, 7)  # a pseudocharge-like field of opposite sign
     tol = 1e-9
     ep = P.EffectivePotential(ctx)
     r = ep.compute(rho, rho_b, poisson_tol=tol)
     veff_o, vxc_o, exc_o, phi_o, it_o = X.effective_potential(H, rho, rho_b, poisson_tol=tol)
     veff, vxc, phi = (t.cpu().numpy() for t in (r.veff, r.vxc, r.phi))
-    assert 6 < r.poisson_iters < 3000
+    assert r.poisson_iters == 0 if direct else 6 < r.poisson_iters < 3000
     assert abs(phi.mean()) < 1e-12
     assert np.abs(vxc - vxc_o).max() <= 1e-11 * np.abs(vxc_o).max()
     assert np.abs(phi - phi_o).max() <= 1e-7 * np.abs(phi_o).max()
     assert np.allclose(veff, vxc + phi, rtol=0, atol=1e-14)
-    # the next call starts from the kept phi and converges at once
-    r2 = ep.compute(rho, rho_b, poisson_tol=tol)
-    assert r2.poisson_iters <= 6
+    rhs = 4 * math.pi * (rho + rho_b)
+    rhs -= rhs.mean()
+    res = np.linalg.norm(rhs - X.neg_laplacian(H, phi)) / np.linalg.norm(rhs)
+    assert res <= (1e-12 if direct else tol)
+    if not direct:
+        # the next call starts from the kept phi and converges at the first check
+        assert ep.compute(rho, rho_b, poisson_tol=tol).poisson_iters <= 6
+    ctx.close()
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("kind", ["periodic", "fcc"])
+def test_direct_poisson_solves_the_discrete_equation(kind):
+    """The FFT solve of a periodic cell (orthogonal, and the non-orthogonal FCC cell with its mixed
+    derivative terms) leaves a residual at rounding level, and for the orthogonal cell agrees with
+    the reference's PoissonSolver run to a tight tolerance."""
+    from lynx_b200 import potential as P
+    ctx, cl, H, rho = _setup(kind)
+    r = P.EffectivePotential(ctx).compute(rho)
+    phi = r.phi.cpu().numpy()
+    rhs = 4 * math.pi * (rho - rho.mean())
+    assert np.linalg.norm(rhs - X.neg_laplacian(H, phi)) <= 1e-12 * np.linalg.norm(rhs)
+    if kind == "periodic":
+        phi_r, _ = ref.RefLynx(cl).poisson(rhs, tol=1e-11)
+        phi_r -= phi_r.mean()
+        assert np.abs(phi - phi_r).max() <= 1e-8 * np.abs(phi_r).max()
     ctx.close()
