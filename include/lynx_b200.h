@@ -199,10 +199,20 @@ LYNX_API int lynx_nonlocal_force_kpt(lynx_ctx* ctx, const double* psi_z, int nba
  * pseudo-random generator (XORWOW) seeded with `seed` fills nband contiguous columns of Nd
  * doubles (2 Nd for complex, real and imaginary interleaved) with uniform values in (0, 1].
  * The reference seeds (spin s, k-point k) with (spin_start + s) * 1000 + (s * Nkpts + k) * 13 + 1.
- * ld must be Nd or 0.  Replaces EigenSolver::randomize_psi_gpu (src/solvers/EigenSolver.hpp:160;
- * src/solvers/EigenSolver.cu:1199-1228) for one (spin, k-point) block. */
+ * ld must be Nd or 0.  A fresh generator per call: the same values as the reference's first
+ * (spin, k-point) block.  Replaces EigenSolver::randomize_psi_gpu (src/solvers/EigenSolver.hpp:160;
+ * src/solvers/EigenSolver.cu:1199-1228) for one block. */
 LYNX_API int lynx_randomize_orbitals(lynx_ctx* ctx, double* psi, int nband, int ld, unsigned long long seed,
                                      int is_complex);
+
+/* All (spin, k-point) blocks as EigenSolver::randomize_psi_gpu(Nspin_local, spin_start, Nkpts)
+ * draws them (src/solvers/EigenSolver.cu:1199-1228): one generator kept across the blocks,
+ * re-seeded per block i = s * nkpts + k with (spin_start + s) * 1000 + i * 13 + 1.  Re-seeding
+ * does not rewind the generator's position, so later blocks differ from a fresh generator with
+ * the same seed; this entry reproduces the reference's draw for every block.  psi[i]: nband
+ * contiguous columns of Nd doubles (2 Nd for complex), i < nspin_local * nkpts. */
+LYNX_API int lynx_randomize_orbitals_all(lynx_ctx* ctx, double** psi, int nspin_local, int spin_start, int nkpts,
+                                         int nband, int is_complex);
 
 /* Kinetic and nonlocal stress of device psi (nband columns, leading dimension ld), before the
  * division by the cell measure, Voigt order xx, xy, xz, yy, yz, zz:

@@ -72,6 +72,7 @@ _SIGNATURES = {
     "lynx_nonlocal_force_kpt": (_c_int, [_p, _p, _c_int, _c_int, _p, ctypes.c_double, _p, _p]),
     "lynx_kinetic_nonlocal_stress": (_c_int, [_p, _p, _c_int, _c_int, _p, ctypes.c_double, _p, _p, _p]),
     "lynx_randomize_orbitals": (_c_int, [_p, _p, _c_int, _c_int, ctypes.c_ulonglong, _c_int]),
+    "lynx_randomize_orbitals_all": (_c_int, [_p, _p, _c_int, _c_int, _c_int, _c_int, _c_int]),
     "lynx_kinetic_nonlocal_stress_kpt": (_c_int, [_p, _p, _c_int, _c_int, _p, ctypes.c_double, _p, _p, _p]),
     "lynx_nonlocal_apply_kpt": (_c_int, [_p, _p, _p, _c_int, _c_int]),
     "lynx_chebyshev_filter": (_c_int, [_p, _p, _p, _p, _c_int, _c_int, _c_double, _c_double, _c_double, _c_int, _c_int]),

@@ -152,6 +152,65 @@ __global__ void hermitize_kernel(double2* A, int N) {
     }
 }
 
+// Complex blocks on the real tensor-core kernels (mixed precision, k-point).  A complex block
+// Y = Yr + i Yi (columns of ld complex elements) is split into the planar real block
+// [Yr | Yi] (2N columns of ld floats); then
+//   [Yr | Yi]^T [Yr | Yi] = [[Yr^T Yr, Yr^T Yi], [Yi^T Yr, Yi^T Yi]]  gives  Y^H Y, and
+//   [Yr | Yi] [[Wr, Wi], [-Wi, Wr]] = [Re(Y W) | Im(Y W)].
+__global__ void planar_kernel(const float2* __restrict__ Y, long long ld, int N, float* __restrict__ P) {
+    const long long total = ld * N;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long j = t / ld, p = t - j * ld;
+        const float2 v = Y[t];
+        P[j * ld + p] = v.x;
+        P[(j + N) * ld + p] = v.y;
+    }
+}
+
+// Complex N x N products from the real 2N x 2N ones (column-major): M (Hermitian, upper triangle
+// from the upper triangle of Mp) and H (all entries from the full Hp):
+//   X(a, b) = Xp(a, b) + Xp(N+a, N+b) + i (Xp(a, N+b) - Xp(N+a, b)).
+__global__ void combine_gram_kernel(const double* __restrict__ Mp, const double* __restrict__ Hp, int N,
+                                    double2* __restrict__ M, double2* __restrict__ H) {
+    const int a = blockIdx.y * blockDim.y + threadIdx.y;
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= N || b >= N) return;
+    const long long n2 = 2LL * N;
+    auto at = [n2](const double* X, long long r, long long c) { return X[r + c * n2]; };
+    H[a + (long long)b * N] =
+        make_double2(at(Hp, a, b) + at(Hp, N + a, N + b), at(Hp, a, N + b) - at(Hp, N + a, b));
+    if (a <= b) {
+        // Mp holds its upper triangle only: Mp(N+a, b) = Mp(b, N+a)
+        M[a + (long long)b * N] =
+            make_double2(at(Mp, a, b) + at(Mp, N + a, N + b), at(Mp, a, N + b) - at(Mp, b, N + a));
+    }
+}
+
+// Wt = [[Wr, Wi], [-Wi, Wr]] (2N x 2N, column-major) from the complex N x N W.
+__global__ void wtilde_kernel(const double2* __restrict__ W, int N, double* __restrict__ Wt) {
+    const int n = blockIdx.y * blockDim.y + threadIdx.y;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N || j >= N) return;
+    const long long n2 = 2LL * N;
+    const double2 w = W[n + (long long)j * N];
+    Wt[n + j * n2] = w.x;
+    Wt[n + (j + N) * n2] = w.y;
+    Wt[(n + N) + j * n2] = -w.y;
+    Wt[(n + N) + (j + N) * n2] = w.x;
+}
+
+// psi[j][p] = (R[j][p], R[N + j][p]) for the Nd points of N columns (R: FP64, column stride Nd).
+__global__ void interleave_kernel(const double* __restrict__ R, long long Nd, int N, double2* __restrict__ psi,
+                                  long long ldp) {
+    const long long total = Nd * N;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long j = t / Nd, p = t - j * Nd;
+        psi[j * ldp + p] = make_double2(R[j * Nd + p], R[(j + N) * Nd + p]);
+    }
+}
+
 // Electron density of one (spin, k-point) block: rho[i] (+)= sum_n w[n] |psi_n(i)|^2, the states in
 // order (src/electronic/ElectronDensity.cpp:85-121, with w[n] = spin factor * k weight * f_n and
 // w[n] = 0 where the reference skips f_n < 1e-16).  One thread per grid point: the reads of every
@@ -249,6 +308,7 @@ struct lynx_ctx {
     DevBuf errflag;         // set by a kernel whose bounded wait gave up
     DevBuf gwork;           // slices, exponents and split partials of the tensor-core Gram
     DevBuf rwork;           // slices and exponents of the tensor-core rotation
+    DevBuf cplx_work;       // planar split and real 2N x 2N products of the mixed k-point Rayleigh-Ritz
     bool no_tc_gram = false;  // diagnostic switch: FP64 library products for the mixed path
     bool autotune = true;     // time the compiled stencil launch shapes on first use per grid
     std::map<std::array<long long, 8>, int> pipe_shape;  // chosen launch shape per (type, grid, columns, fused, xold)
@@ -1110,24 +1170,25 @@ int rayleigh_ritz_mixed_real(lynx_ctx* c, const float* Y32, const float* HY32, l
     return rr_subspace_real(c, c->cvt[0].as<double>(), Nd, psi, ldp, N, eig_host);
 }
 
-int rayleigh_ritz_cplx(lynx_ctx* c, const double2* Y, long long ldY, const double2* HY, long long ldH,
-                       double2* psi, long long ldp, int N, double* eig_host) {
+int rr_alloc_small_cplx(lynx_ctx* c, int N) {
     const size_t nn = (size_t)N * N;
     LYNX_TRY(c->Ms.ensure(nn * sizeof(double2)));
     LYNX_TRY(c->Hs.ensure(nn * sizeof(double2)));
     LYNX_TRY(c->eigd.ensure(N * sizeof(double)));
     LYNX_TRY(c->info.ensure(3 * sizeof(int)));
-    cuDoubleComplex* Ms = c->Ms.as<cuDoubleComplex>();
-    cuDoubleComplex* Hs = c->Hs.as<cuDoubleComplex>();
-    const cuDoubleComplex* Yz = reinterpret_cast<const cuDoubleComplex*>(Y);
-    const cuDoubleComplex* HYz = reinterpret_cast<const cuDoubleComplex*>(HY);
-    const double dV = c->dV, zero_r = 0.0;
-    const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0),
-                          dVz = make_cuDoubleComplex(dV, 0);
     CUBLAS_TRY(cublasSetStream(c->cublas, c->stream));
     CUSOLVER_TRY(cusolverDnSetStream(c->cusolver, c->stream));
-    CUBLAS_TRY(cublasZherk(c->cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, N, c->Nd, &dV, Yz, ldY, &zero_r, Ms, N));
-    CUBLAS_TRY(cublasZgemm(c->cublas, CUBLAS_OP_C, CUBLAS_OP_N, N, N, c->Nd, &dVz, Yz, ldY, HYz, ldH, &zero, Hs, N));
+    LYNX_CUDA_TRY(cudaMemsetAsync(c->info.p, 0, 3 * sizeof(int), c->stream));
+    return LYNX_OK;
+}
+
+// Subspace part of the complex Rayleigh-Ritz step, given Ms = dV Y^H Y (upper triangle) and
+// Hs = dV Y^H HY in c->Ms / c->Hs: Hs' = R^-H herm(Hs) R^-1 with R^H R = Ms, eigenpairs of Hs'
+// (values into c->eigd), W = R^-1 Q left in c->Hs.  Asynchronous.
+int rr_small_cplx(lynx_ctx* c, int N) {
+    cuDoubleComplex* Ms = c->Ms.as<cuDoubleComplex>();
+    cuDoubleComplex* Hs = c->Hs.as<cuDoubleComplex>();
+    const cuDoubleComplex one = make_cuDoubleComplex(1, 0);
     {
         dim3 b(16, 16), g((N + 15) / 16, (N + 15) / 16);
         hermitize_kernel<<<g, b, 0, c->stream>>>(reinterpret_cast<double2*>(Hs), N);
@@ -1141,7 +1202,6 @@ int rayleigh_ritz_cplx(lynx_ctx* c, const double2* Y, long long ldY, const doubl
     LYNX_TRY(c->solver_work.ensure((size_t)lw * sizeof(cuDoubleComplex)));
     int* info = c->info.as<int>();
     cuDoubleComplex* work = c->solver_work.as<cuDoubleComplex>();
-    LYNX_CUDA_TRY(cudaMemsetAsync(info, 0, 3 * sizeof(int), c->stream));
     LYNX_TRY(check_finite(c, reinterpret_cast<const double*>(Ms), N, 2, true, info + 2));
     LYNX_TRY(check_finite(c, reinterpret_cast<const double*>(Hs), N, 2, false, info + 2));
     CUSOLVER_TRY(cusolverDnZpotrf(c->cusolver, CUBLAS_FILL_MODE_UPPER, N, Ms, N, work, lw, info));
@@ -1153,8 +1213,75 @@ int rayleigh_ritz_cplx(lynx_ctx* c, const double2* Y, long long ldY, const doubl
                                   c->eigd.as<double>(), work, lw, info + 1));
     CUBLAS_TRY(cublasZtrsm(c->cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT,
                            N, N, &one, Ms, N, Hs, N));
+    return LYNX_OK;
+}
+
+int rayleigh_ritz_cplx(lynx_ctx* c, const double2* Y, long long ldY, const double2* HY, long long ldH,
+                       double2* psi, long long ldp, int N, double* eig_host) {
+    LYNX_TRY(rr_alloc_small_cplx(c, N));
+    cuDoubleComplex* Ms = c->Ms.as<cuDoubleComplex>();
+    cuDoubleComplex* Hs = c->Hs.as<cuDoubleComplex>();
+    const cuDoubleComplex* Yz = reinterpret_cast<const cuDoubleComplex*>(Y);
+    const cuDoubleComplex* HYz = reinterpret_cast<const cuDoubleComplex*>(HY);
+    const double dV = c->dV, zero_r = 0.0;
+    const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0),
+                          dVz = make_cuDoubleComplex(dV, 0);
+    CUBLAS_TRY(cublasZherk(c->cublas, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_C, N, c->Nd, &dV, Yz, ldY, &zero_r, Ms, N));
+    CUBLAS_TRY(cublasZgemm(c->cublas, CUBLAS_OP_C, CUBLAS_OP_N, N, N, c->Nd, &dVz, Yz, ldY, HYz, ldH, &zero, Hs, N));
+    LYNX_TRY(rr_small_cplx(c, N));
     CUBLAS_TRY(cublasZgemm(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, c->Nd, N, N, &one, Yz, ldY, Hs, N, &zero,
                            reinterpret_cast<cuDoubleComplex*>(psi), ldp));
+    return finish_rr(c, N, eig_host);
+}
+
+// Mixed precision, k-point: the Gram products and the rotation of the FP32 complex blocks on the
+// real tensor-core kernels, through the planar split [Yr | Yi] (2N real states); subspace algebra
+// in complex FP64.
+int rayleigh_ritz_mixed_cplx(lynx_ctx* c, const float2* Y32, const float2* HY32, long long ldb, int nxp,
+                             double2* psi, long long ldp, int N, double* eig_host) {
+    const int N2 = 2 * N;
+    const long long Nd = c->Nd;
+    LYNX_TRY(rr_alloc_small_cplx(c, N));
+    // planar copies of Y and HY, the real 2N x 2N products, Wt, and the planar FP64 rotation output
+    const size_t pl_bytes = sizeof(float) * (size_t)ldb * N2;
+    const size_t sq_bytes = sizeof(double) * (size_t)N2 * N2;
+    LYNX_TRY(c->cplx_work.ensure(2 * pl_bytes + 3 * sq_bytes));
+    float* Yp = reinterpret_cast<float*>(c->cplx_work.p);
+    float* Hp = Yp + (size_t)ldb * N2;
+    double* Mpl = reinterpret_cast<double*>(reinterpret_cast<unsigned char*>(c->cplx_work.p) + 2 * pl_bytes);
+    double* Hpl = Mpl + (size_t)N2 * N2;
+    double* Wt = Hpl + (size_t)N2 * N2;
+    LYNX_TRY(c->cvt[0].ensure(sizeof(double) * (size_t)Nd * N2));
+    double* R = c->cvt[0].as<double>();
+    const int blocks = (int)std::min<long long>((ldb * N + 255) / 256, 148LL * 16);
+    planar_kernel<<<blocks, 256, 0, c->stream>>>(Y32, ldb, N, Yp);
+    planar_kernel<<<blocks, 256, 0, c->stream>>>(HY32, ldb, N, Hp);
+    count_launch(2);
+    const GramPlan plan = gram_plan(ldb, N2);  // all ldb rows: pad elements are zero
+    LYNX_TRY(c->gwork.ensure(plan.work_bytes));
+    if (!c->errflag.p) LYNX_TRY(ensure_zeroed(c, c->errflag, sizeof(int)));
+    LYNX_TRY(launch_gram_i8(Yp, Hp, ldb, ldb, N2, c->dV, plan, c->gwork.p, c->gwork.bytes, Mpl, Hpl,
+                            c->errflag.as<int>(), c->info.as<int>() + 2, c->stream));
+    const RotPlan rp = rot_plan(ldb, N2);
+    LYNX_TRY(c->rwork.ensure(rp.work_bytes));
+    LYNX_TRY(launch_colexp(Mpl, N2, c->rwork.p, rp, ldb, c->stream));  // scaling of the 2N planar states
+    {
+        dim3 b(16, 16), g((N + 15) / 16, (N + 15) / 16);
+        combine_gram_kernel<<<g, b, 0, c->stream>>>(Mpl, Hpl, N, c->Ms.as<double2>(), c->Hs.as<double2>());
+        count_launch();
+    }
+    LYNX_TRY(rr_small_cplx(c, N));
+    {
+        dim3 b(16, 16), g((N + 15) / 16, (N + 15) / 16);
+        wtilde_kernel<<<g, b, 0, c->stream>>>(c->Hs.as<double2>(), N, Wt);
+        count_launch();
+    }
+    LYNX_TRY(launch_rot_i8(Yp, ldb, ldb, c->nx, nxp, Wt, N2, rp, c->rwork.p, c->rwork.bytes, R, Nd,
+                           c->errflag.as<int>(), c->stream));
+    const int ib = (int)std::min<long long>((Nd * N + 255) / 256, 148LL * 16);
+    interleave_kernel<<<ib, 256, 0, c->stream>>>(R, Nd, N, psi, ldp);
+    count_launch();
+    LYNX_CUDA_TRY(cudaGetLastError());
     return finish_rr(c, N, eig_host);
 }
 
@@ -1205,6 +1332,13 @@ int solve_impl(lynx_ctx* c, T64* psi, double* eig, const double* veff, int N, in
         if constexpr (std::is_same<T32, float>::value) {
             if (pipe_capable<float>(c->nx) && !c->no_tc_gram) {
                 LYNX_TRY(rayleigh_ritz_mixed_real(c, Y, HY, ldb, nxp, reinterpret_cast<double*>(psi), ldp, N, eig));
+                LYNX_TRY(check_errflag(c));
+                if (lc_out) *lc_out = eig[N - 1] + 0.1;
+                return LYNX_OK;
+            }
+        } else {
+            if (pipe_capable<float>(c->nx) && rot_supported(2 * N) && !c->no_tc_gram) {
+                LYNX_TRY(rayleigh_ritz_mixed_cplx(c, Y, HY, ldb, nxp, reinterpret_cast<double2*>(psi), ldp, N, eig));
                 LYNX_TRY(check_errflag(c));
                 if (lc_out) *lc_out = eig[N - 1] + 0.1;
                 return LYNX_OK;
@@ -1529,7 +1663,7 @@ int lynx_destroy(lynx_ctx* c) {
         kv.second.ptmap.release();
         kv.second.rowstart.release();
     }
-    for (DevBuf* b : {&c->dens_w, &c->dens_part, &c->vwork, &c->vzero, &c->vones, &c->dotw, &c->xcwork, &c->fft_sym,
+    for (DevBuf* b : {&c->cplx_work, &c->dens_w, &c->dens_part, &c->vwork, &c->vzero, &c->vones, &c->dotw, &c->xcwork, &c->fft_sym,
                       &c->fft_z})
         b->release();
     if (c->fft_ready) {
@@ -2345,6 +2479,34 @@ extern "C" int lynx_randomize_orbitals(lynx_ctx* c, double* psi, int nband, int 
     curandStatus_t r = curandSetStream(g, c->stream);
     if (r == CURAND_STATUS_SUCCESS) r = curandSetPseudoRandomGeneratorSeed(g, seed);
     if (r == CURAND_STATUS_SUCCESS) r = curandGenerateUniformDouble(g, psi, n);
+    curandDestroyGenerator(g);
+    if (r != CURAND_STATUS_SUCCESS) {
+        set_error("cuRAND uniform generation failed (status %d)", (int)r);
+        return LYNX_ERR_CUDA;
+    }
+    return LYNX_OK;
+}
+
+extern "C" int lynx_randomize_orbitals_all(lynx_ctx* c, double** psi, int nspin_local, int spin_start, int nkpts,
+                                           int nband, int is_complex) {
+    LYNX_CHECK_ARG(c && psi, "null pointer");
+    LYNX_CHECK_ARG(nband > 0 && nspin_local > 0 && nkpts > 0, "block counts must be positive");
+    const int nsk = nspin_local * nkpts;
+    for (int i = 0; i < nsk; ++i) LYNX_CHECK_ARG(psi[i] != nullptr, "null block pointer");
+    LYNX_TRY(activate(c));
+    curandGenerator_t g = nullptr;
+    if (curandCreateGenerator(&g, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS) {
+        set_error("curandCreateGenerator failed");
+        return LYNX_ERR_CUDA;
+    }
+    const size_t n = (size_t)c->Nd * nband * (is_complex ? 2 : 1);
+    curandStatus_t r = curandSetStream(g, c->stream);
+    for (int i = 0; i < nsk && r == CURAND_STATUS_SUCCESS; ++i) {
+        const int s = i / nkpts;
+        const unsigned long long seed = (unsigned long long)(spin_start + s) * 1000ULL + (unsigned long long)i * 13ULL + 1ULL;
+        r = curandSetPseudoRandomGeneratorSeed(g, seed);
+        if (r == CURAND_STATUS_SUCCESS) r = curandGenerateUniformDouble(g, psi[i], n);
+    }
     curandDestroyGenerator(g);
     if (r != CURAND_STATUS_SUCCESS) {
         set_error("cuRAND uniform generation failed (status %d)", (int)r);

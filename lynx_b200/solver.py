@@ -428,6 +428,24 @@ def randomize_orbitals(ctx: Context, nband: int, seed: int, complex_: bool = Fal
     return torch.view_as_complex(t.view(nband, ctx.nd, 2)) if complex_ else t
 
 
+def randomize_orbitals_all(ctx: Context, nband: int, nspin_local: int, nkpts: int, spin_start: int = 0,
+                           complex_: bool = False):
+    """Every (spin, k-point) block as EigenSolver::randomize_psi_gpu draws them, one generator
+    kept across the blocks (lynx_randomize_orbitals_all): a list of nspin_local * nkpts tensors
+    (nband, Nd), float64 or complex128, block i = s * nkpts + k."""
+    torch = _torch()
+    ctx.sync_stream()
+    nsk = nspin_local * nkpts
+    w = ctx.nd * (2 if complex_ else 1)
+    ts = [torch.empty((nband, w), dtype=torch.float64, device=f"cuda:{ctx.device}") for _ in range(nsk)]
+    ptrs = (ctypes.c_void_p * nsk)(*[t.data_ptr() for t in ts])
+    check(ctx.lib.lynx_randomize_orbitals_all(ctx.handle, ptrs, int(nspin_local), int(spin_start), int(nkpts),
+                                              int(nband), 1 if complex_ else 0))
+    if complex_:
+        return [torch.view_as_complex(t.view(nband, ctx.nd, 2)) for t in ts]
+    return ts
+
+
 def solve_batch(solvers, psis, Veffs, lambda_cutoffs, eigval_mins, eigval_maxs, cheb_degree: int = 20,
                 precision: Optional[str] = None, kpt=False):
     """One CheFSI pass of several independent problems at once (lynx_eigensolver_solve_batch).
