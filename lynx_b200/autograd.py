@@ -1,9 +1,16 @@
 """Differentiable operators for PyTorch (torch.autograd.Function), on top of the C ABI.
 
-* ``hamiltonian_apply(ctx, psi, veff)``: y = H psi with H = -0.5 Lap + Veff + Vnl (real, Gamma
-  point).  H is symmetric on the grid (symmetric FD stencil, diagonal Veff, Vnl = dV chi Gamma
-  chi^T), so the adjoint with respect to the orbitals is H itself, grad_psi = H grad_y, and with
-  respect to the potential grad_Veff = sum_n grad_y_n * psi_n.
+* ``hamiltonian_apply(ctx, psi, veff, positions=None, psp=None)``: y = H psi with H = -0.5 Lap +
+  Veff + Vnl (real, Gamma point).  H is symmetric on the grid (symmetric FD stencil, diagonal
+  Veff, Vnl = dV chi Gamma chi^T), so the adjoint with respect to the orbitals is H itself,
+  grad_psi = H grad_y, and with respect to the potential grad_Veff = sum_n grad_y_n * psi_n.
+  With atom positions (and ``psp`` to rebuild the tables there) the positions are an input too:
+  for L = sum_n <g_n, Vnl psi_n> = (1/dV) sum_n a(g_n)^T Gamma a(psi_n), a(x) = dV chi^T x,
+  dL/dR = (1/dV) sum_n sum_p Gamma_p [b(g_n) a(psi_n) + a(g_n) b(psi_n)]_p with b = da/dR, the
+  projection of the FD gradient used by the nonlocal forces.  By the polarisation identity
+  a(u)b(v) + a(v)b(u) = (a(u+v)b(u+v) - a(u-v)b(u-v)) / 2, that is two calls of the force kernel
+  (lynx_nonlocal_force, F(x) = -2 sum_n sum_p Gamma_p a(x_n) b(x_n) with unit occupations):
+  grad_R = (F(psi - g) - F(psi + g)) / (4 dV).
 * ``nonlocal_energy(ctx, psi, positions, occ, occfac, psp)``: E_nl = occfac sum_n f_n sum_p
   Gamma_p alpha_{p,n}^2 (alpha = dV chi^T psi_n); grad_psi_n = 2 occfac f_n dV (Vnl psi_n)
   (d alpha / d psi = dV chi, and Vnl psi = chi Gamma alpha), and grad_positions = -F with F the
@@ -34,9 +41,14 @@ def _make_fns():
 
     class HamiltonianApply(torch.autograd.Function):
         @staticmethod
-        def forward(fctx, psi, veff, ctx):
+        def forward(fctx, psi, veff, positions, ctx, psp):
+            if psp is not None and positions is not None:
+                from . import pseudo
+                R = positions.detach().cpu().numpy().astype(np.float64)
+                ctx.set_nonlocal(pseudo.nonlocal_tables(ctx.cell, R, psp))
             fctx.ctx = ctx
             fctx.save_for_backward(psi, veff)
+            fctx.pos_like = positions
             return solver.Hamiltonian(ctx).apply(psi.contiguous(), Veff=veff.contiguous())
 
         @staticmethod
@@ -45,7 +57,16 @@ def _make_fns():
             g = grad_y.contiguous()
             grad_psi = solver.Hamiltonian(fctx.ctx).apply(g, Veff=veff.contiguous()) if fctx.needs_input_grad[0] else None
             grad_v = (g * psi).sum(0) if fctx.needs_input_grad[1] else None
-            return grad_psi, grad_v, None
+            grad_pos = None
+            if fctx.needs_input_grad[2]:
+                ones = np.ones(psi.shape[0])
+                nl = solver.NonlocalProjector(fctx.ctx)
+                fm, _ = nl.force((psi - g).contiguous(), ones, occfac=1.0)
+                fp, _ = nl.force((psi + g).contiguous(), ones, occfac=1.0)
+                pos = fctx.pos_like
+                grad_pos = torch.as_tensor((np.asarray(fm) - np.asarray(fp)) / (4.0 * fctx.ctx.dV),
+                                           dtype=pos.dtype, device=pos.device).reshape(pos.shape)
+            return grad_psi, grad_v, grad_pos, None, None
 
     class NonlocalEnergy(torch.autograd.Function):
         @staticmethod
@@ -89,9 +110,10 @@ def _fns():
     return _FNS
 
 
-def hamiltonian_apply(ctx, psi, veff):
-    """y = H psi, differentiable in psi and veff (see the module docstring)."""
-    return _fns()[0].apply(psi, veff, ctx)
+def hamiltonian_apply(ctx, psi, veff, positions=None, psp=None):
+    """y = H psi, differentiable in psi, veff and (when given) the atom positions; with ``psp`` the
+    projector tables are rebuilt at ``positions`` first (see the module docstring)."""
+    return _fns()[0].apply(psi, veff, positions, ctx, psp)
 
 
 def nonlocal_energy(ctx, psi, positions, occ, occfac: float = 2.0, psp=None):

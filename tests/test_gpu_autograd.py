@@ -2,11 +2,12 @@
 * H psi: the loss L = <w, H(psi, V)> is linear in psi and in V, so a central difference along a
   random direction equals the gradient's directional derivative up to rounding (1e-9 relative);
 * E_nl: quadratic in psi, so the central difference is again exact up to rounding;
-* E_nl in the atom positions, with the projector tables rebuilt at every displaced position: the
-  gradient (minus the nonlocal force of src/physics/Forces.cpp:509-797) against the GPU central
-  difference of E_nl(R +- h), h = 1e-3 Bohr.  The force formula projects the FD gradient of psi
-  (summation by parts) while the difference moves the sampled projector, so they agree to the
-  grid discretisation of the projector gradient: 1e-3 relative, as for the CPU oracle's pin."""
+* E_nl and <w, H psi> in the atom positions, with the projector tables rebuilt at every
+  displaced position: the gradients (for E_nl minus the nonlocal force of
+  src/physics/Forces.cpp:509-797) against the GPU central differences at R +- h, h = 1e-3 Bohr.
+  The force formula projects the FD gradient of psi (summation by parts) while the difference
+  moves the sampled projector, so they agree to the grid discretisation of the projector
+  gradient: 1e-3 relative, as for the CPU oracle's pin."""
 import numpy as np
 import pytest
 
@@ -102,4 +103,56 @@ def test_nonlocal_energy_position_gradient_central_difference(synth_psp8):
             e.append(float(nonlocal_energy(ctx, psi, p2, occ, 2.0, psp)))
         fd = (e[0] - e[1]) / (2 * h)
         assert abs(fd) > 0.1 and abs(grad[atom, dim] - fd) <= 1e-3 * abs(fd), (atom, dim, grad[atom, dim], fd)
+    ctx.close()
+
+
+def test_hamiltonian_position_adjoint_central_difference(synth_psp8):
+    """The position adjoint of H psi: for L = <w, H(R) psi> the gradient in the atom positions
+    against L(R +- h) on the GPU with the projector tables rebuilt at every displaced position
+    (h = 1e-3 Bohr).  The adjoint projects FD gradients (summation by parts), so it agrees with the
+    difference to the grid discretisation of the projector gradient: 1e-3 relative."""
+    import torch
+    from lynx_b200 import solver
+    from lynx_b200.autograd import hamiltonian_apply
+    psp = P.read_psp8(synth_psp8)
+    cl, pos = C.diamond_si(1, 24, displace=0.05, seed=11)
+    ctx = solver.Context(cl)
+    rng = np.random.default_rng(5)
+    pts = cl.grid_points_cart()
+
+    def smooth(n):
+        out = np.zeros((n, ctx.nd))
+        for i in range(n):
+            for _ in range(6):
+                kv = 2 * np.pi * rng.integers(-2, 3, size=3) / cl.lengths
+                out[i] += rng.normal() * np.cos(pts @ kv + rng.uniform(0, 2 * np.pi))
+        return out
+
+    psi = _dev(torch, smooth(3))
+    w = _dev(torch, smooth(3))
+    V = _dev(torch, np.zeros(ctx.nd))
+    R = torch.tensor(pos, dtype=torch.float64, requires_grad=True)
+    L = (w * hamiltonian_apply(ctx, psi, V, R, psp)).sum()
+    L.backward()
+    grad = R.grad.numpy()
+    h = 1e-3
+    checked = 0
+    for atom in range(len(pos)):
+        for dim in range(3):
+            e = []
+            for sgn in (1, -1):
+                p2 = torch.tensor(pos, dtype=torch.float64)
+                p2[atom, dim] += sgn * h
+                with torch.no_grad():
+                    e.append(float((w * hamiltonian_apply(ctx, psi, V, p2, psp)).sum()))
+            fd = (e[0] - e[1]) / (2 * h)
+            if abs(fd) < 0.05:
+                continue
+            checked += 1
+            assert abs(grad[atom, dim] - fd) <= 1e-3 * abs(fd), (atom, dim, grad[atom, dim], fd)
+            if checked >= 4:
+                break
+        if checked >= 4:
+            break
+    assert checked >= 4
     ctx.close()
