@@ -21,6 +21,15 @@
   function of the positions; without one, the context's current tables are used and must
   belong to ``positions``.  The position gradient is along the lattice directions (Cartesian
   for orthogonal cells).
+* ``strain_energy(cell, positions, psp, psi, occ, strain, occfac)``: the kinetic + nonlocal
+  band energy under a homogeneous diagonal strain of an orthogonal cell (grid, atoms and cell
+  stretch by 1 + strain[a] along axis a; the orbitals keep their grid values, rescaled to keep
+  their norm), differentiable in the strain: E = E_k + E_nl with E_k = 1/2 occfac sum_n f_n
+  dV |D psi_n|^2 (D the FD gradient: minus half the trace of the kinetic stress) and E_nl from
+  the projector tables rebuilt in the strained cell; dE/dstrain[a] = (stress_k[aa] +
+  stress_nl[aa]) / (1 + strain[a]) with the stress of lynx_kinetic_nonlocal_stress in the
+  strained cell (before the division by the cell measure; the formula of the reference's
+  Stress::compute_nonlocal_kinetic, src/physics/Stress.cpp:1041-1784).
 
 Orbitals are torch CUDA tensors of shape (ncol, Nd), float64 (the layout lynx_b200.solver takes
 without copies); the computation runs in liblynxb200.so.
@@ -97,7 +106,35 @@ def _make_fns():
                 grad_pos = -grad_e.to(device=fctx.force.device, dtype=fctx.force.dtype) * fctx.force
             return grad_psi, grad_pos, None, None, None, None
 
-    return HamiltonianApply, NonlocalEnergy
+    class StrainEnergy(torch.autograd.Function):
+        @staticmethod
+        def forward(fctx, strain, cell, positions, psp, psi, occ, occfac):
+            from . import pseudo
+            from .cell import Cell
+            f = 1.0 + strain.detach().cpu().numpy().astype(np.float64).reshape(3)
+            cl2 = Cell(np.asarray(cell.latvec) * f[None, :], cell.shape, True, tuple(cell.bc), cell.fd_order)
+            ctx2 = solver.Context(cl2, device=psi.device.index or 0)
+            try:
+                ctx2.set_nonlocal(pseudo.nonlocal_tables(cl2, np.asarray(positions, dtype=np.float64) * f[None, :], psp))
+                psi2 = (psi * float(np.prod(f)) ** -0.5).contiguous()
+                occ = np.asarray(occ, dtype=np.float64)
+                nl = solver.NonlocalProjector(ctx2)
+                sk, snl = nl.stress(psi2, occ, occfac=occfac)
+                _, enl = nl.force(psi2, occ, occfac=occfac)
+            finally:
+                ctx2.close()
+            # the stress is the derivative in a strain of the strained cell; one more strain d of it
+            # is a change of (1 + strain[a]) (1 + d): d/dstrain[a] = stress[aa] / (1 + strain[a])
+            fctx.grad = torch.tensor([(sk[0] + snl[0]) / f[0], (sk[3] + snl[3]) / f[1], (sk[5] + snl[5]) / f[2]],
+                                     dtype=strain.dtype, device=strain.device)
+            e = -0.5 * (sk[0] + sk[3] + sk[5]) + enl
+            return torch.tensor(e, dtype=strain.dtype, device=strain.device)
+
+        @staticmethod
+        def backward(fctx, grad_e):
+            return grad_e * fctx.grad, None, None, None, None, None, None
+
+    return HamiltonianApply, NonlocalEnergy, StrainEnergy
 
 
 _FNS = None
@@ -120,3 +157,12 @@ def nonlocal_energy(ctx, psi, positions, occ, occfac: float = 2.0, psp=None):
     """E_nl of the orbitals psi, differentiable in psi and in the atom positions (with ``psp``,
     a lynx_b200.pseudo.Psp8, the projector tables are rebuilt at ``positions`` first)."""
     return _fns()[1].apply(psi, positions, ctx, occ, occfac, psp)
+
+
+def strain_energy(cell, positions, psp, psi, occ, strain, occfac: float = 2.0):
+    """Kinetic + nonlocal band energy of psi in the cell stretched by 1 + strain[a] along each axis
+    (orthogonal cells), differentiable in ``strain`` (a torch tensor of 3 values); the gradient is
+    the diagonal of the kinetic + nonlocal stress (see the module docstring)."""
+    if not cell.orthogonal:
+        raise ValueError("strain_energy takes orthogonal cells (diagonal strain)")
+    return _fns()[2].apply(strain, cell, positions, psp, psi, occ, occfac)

@@ -7,7 +7,9 @@
   src/physics/Forces.cpp:509-797) against the GPU central differences at R +- h, h = 1e-3 Bohr.
   The force formula projects the FD gradient of psi (summation by parts) while the difference
   moves the sampled projector, so they agree to the grid discretisation of the projector
-  gradient: 1e-3 relative, as for the CPU oracle's pin."""
+  gradient: 1e-3 relative, as for the CPU oracle's pin;
+* the kinetic + nonlocal energy in a diagonal strain: its gradient (the stress diagonal) against
+  central differences of the energy in strained cells."""
 import numpy as np
 import pytest
 
@@ -156,3 +158,37 @@ def test_hamiltonian_position_adjoint_central_difference(synth_psp8):
             break
     assert checked >= 4
     ctx.close()
+
+
+def test_strain_energy_gradient_central_difference(synth_psp8):
+    """The strain adjoint: d(E_k + E_nl)/d strain[a] (the diagonal of the GPU kinetic + nonlocal
+    stress, in the strained cell) against central differences of the energy at strain +- h
+    (h = 1e-4), the projector tables rebuilt in each strained cell.  The kinetic part is exact up
+    to the difference's O(h^2); the nonlocal part agrees to the grid discretisation of the
+    summation by parts with the FD gradient: 1e-3 relative."""
+    import torch
+    from lynx_b200.autograd import strain_energy
+    psp = P.read_psp8(synth_psp8)
+    cl, pos = C.diamond_si(1, 24, displace=0.05, seed=11)
+    rng = np.random.default_rng(9)
+    pts = cl.grid_points_cart()
+    psi_h = np.zeros((3, cl.nd))
+    for n in range(3):
+        for _ in range(6):
+            kv = 2 * np.pi * rng.integers(-2, 3, size=3) / cl.lengths
+            psi_h[n] += rng.normal() * np.cos(pts @ kv + rng.uniform(0, 2 * np.pi))
+    psi = _dev(torch, psi_h)
+    occ = np.array([1.0, 0.6, 0.25])
+    eps = torch.tensor([0.004, -0.006, 0.002], dtype=torch.float64, requires_grad=True)
+    E = strain_energy(cl, pos, psp, psi, occ, eps)
+    E.backward()
+    grad = eps.grad.numpy()
+    h = 1e-4
+    for a in range(3):
+        e = []
+        for sgn in (1, -1):
+            e2 = eps.detach().clone()
+            e2[a] += sgn * h
+            e.append(float(strain_energy(cl, pos, psp, psi, occ, e2)))
+        fd = (e[0] - e[1]) / (2 * h)
+        assert abs(fd) > 1.0 and abs(grad[a] - fd) <= 1e-3 * abs(fd), (a, grad[a], fd)
