@@ -367,13 +367,20 @@ LYNX_API int lynx_nonlocal_apply_noalloc(lynx_ctx* ctx, const double* psi, doubl
  *                            of a periodic cell exactly by FFT (the discrete equation the AAR
  *                            iteration converges to, to rounding); 0 uses the AAR iteration.
  *                            lynx_poisson_solve is always the AAR iteration.
+ *   LYNX_OPT_STENCIL_SHAPE:  0 (default) leaves the stencil launch shape to LYNX_OPT_AUTOTUNE;
+ *                            k >= 1 makes every pipelined stencil launch use compiled shape k - 1
+ *                            (a diagnostic for timing the shapes one by one; an index past the
+ *                            compiled shapes selects the default shape, and a shape whose stages
+ *                            do not fit the grid fails with LYNX_ERR_UNSUPPORTED).  Same results,
+ *                            bitwise.
  */
 enum {
     LYNX_OPT_AUTOTUNE = 1,
     LYNX_OPT_FUSE_NONLOCAL = 2,
     LYNX_OPT_TC_RAYLEIGH_RITZ = 3,
     LYNX_OPT_COMPACT_GATHER = 4,
-    LYNX_OPT_POISSON_DIRECT = 5
+    LYNX_OPT_POISSON_DIRECT = 5,
+    LYNX_OPT_STENCIL_SHAPE = 6
 };
 LYNX_API int lynx_set_option(lynx_ctx* ctx, int option, int value);
 

@@ -311,6 +311,7 @@ struct lynx_ctx {
     DevBuf cplx_work;       // planar split and real 2N x 2N products of the mixed k-point Rayleigh-Ritz
     bool no_tc_gram = false;  // diagnostic switch: FP64 library products for the mixed path
     bool autotune = true;     // time the compiled stencil launch shapes on first use per grid
+    int force_shape = -1;     // diagnostic: compiled stencil launch shape used for every launch
     std::map<std::array<long long, 8>, int> pipe_shape;  // chosen launch shape per (type, grid, columns, fused, xold)
     bool fuse_nl = true;      // add the nonlocal term inside the stencil when the spheres are disjoint
     // with fuse_nl: the stencil also writes compact sphere-point copies of its output and the
@@ -719,6 +720,9 @@ int pipe_launch_tuned(lynx_ctx* c, int nxp, const T* x, long long ldx, const T* 
     const int nsh = pipe_shape_count<T>(g.R);
     const std::array<long long, 8> key = {(long long)sizeof(T), (long long)ScalarOf<T>::cplx, nxp, c->ny, c->nz,
                                           ncol, nlh != nullptr, xold != nullptr && d != 0.0};
+    if (c->force_shape >= 0)
+        return launch_cheb_pipe<T, S>(g, nxp, x, ldx, xold, ldo, out, ldout, V, ncol, a, b, d, phl, phr,
+                                      c->errflag.as<int>(), c->stream, c->force_shape < nsh ? c->force_shape : 0, nlh);
     auto it = c->pipe_shape.find(key);
     if (it != c->pipe_shape.end() || nsh <= 1 || !c->autotune) {
         const int si = (it != c->pipe_shape.end()) ? it->second : 0;
@@ -2561,6 +2565,7 @@ extern "C" int lynx_set_option(lynx_ctx* c, int option, int value) {
         case LYNX_OPT_TC_RAYLEIGH_RITZ: c->no_tc_gram = value == 0; return LYNX_OK;
         case LYNX_OPT_COMPACT_GATHER: c->fuse_compact_gather = value != 0; return LYNX_OK;
         case LYNX_OPT_POISSON_DIRECT: c->poisson_direct = value != 0; return LYNX_OK;
+        case LYNX_OPT_STENCIL_SHAPE: c->force_shape = value > 0 ? value - 1 : -1; return LYNX_OK;
         default: set_error("unknown option %d", option); return LYNX_ERR_BAD_ARG;
     }
 }

@@ -271,6 +271,29 @@ def test_fused_nonlocal_and_shapes_bitwise(system):
             assert np.array_equal(out[key + (prec,)], ref_), (key, prec)
 
 
+def test_fused_nonlocal_wide_rows_bitwise(synth_psp8):
+    """A wider grid (36 x 20 x 40) whose z extent recycles every ring stage of the fused stencil
+    several times, each stage carrying a different W range: the fused term and its compact copy
+    give bitwise the separate-scatter results in both precisions."""
+    from lynx_b200 import _lib, solver
+    cl, pos, V = si8_small(grid=(36, 20, 40), seed=5)
+    X = C.random_orbitals(int(np.prod(cl.shape)), 12, seed=93)
+    out = {}
+    for fuse, compact in ((0, 0), (1, 0), (1, 1)):
+        ctx = solver.Context(cl)
+        ctx.set_nonlocal(P.nonlocal_tables(cl, pos, P.read_psp8(synth_psp8)))
+        _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_FUSE_NONLOCAL, fuse))
+        _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_COMPACT_GATHER, compact))
+        es = solver.EigenSolver(ctx)
+        lo, hi = es.lanczos_bounds(V)
+        for prec in ("fp64", "mixed"):
+            out[(fuse, compact, prec)] = es.chebyshev_filter(X, V, 0.5 * (lo + hi), lo, hi, 5, precision=prec)
+        ctx.close()
+    for prec in ("fp64", "mixed"):
+        for key in ((1, 0), (1, 1)):
+            assert np.array_equal(out[key + (prec,)], out[(0, 0, prec)]), (key, prec)
+
+
 def test_host_solve_pipelined_matches_device(system):
     """lynx_eigensolver_solve_host copies psi in column blocks on a second stream and filters
     each block as it lands (mixed precision, >= 256 states): bitwise the device-pointer pass."""
