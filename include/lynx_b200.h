@@ -373,6 +373,10 @@ LYNX_API int lynx_nonlocal_apply_noalloc(lynx_ctx* ctx, const double* psi, doubl
  *                            compiled shapes selects the default shape, and a shape whose stages
  *                            do not fit the grid fails with LYNX_ERR_UNSUPPORTED).  Same results,
  *                            bitwise.
+ *   LYNX_OPT_HOST_COPY_BLOCK: columns per block of the pipelined host-to-device copy of
+ *                            lynx_eigensolver_solve_host (mixed precision, >= 256 states): 0 or
+ *                            less restores the default (128); the filter starts on a block as
+ *                            soon as it has landed.  Same results, bitwise.
  */
 enum {
     LYNX_OPT_AUTOTUNE = 1,
@@ -380,7 +384,8 @@ enum {
     LYNX_OPT_TC_RAYLEIGH_RITZ = 3,
     LYNX_OPT_COMPACT_GATHER = 4,
     LYNX_OPT_POISSON_DIRECT = 5,
-    LYNX_OPT_STENCIL_SHAPE = 6
+    LYNX_OPT_STENCIL_SHAPE = 6,
+    LYNX_OPT_HOST_COPY_BLOCK = 7
 };
 LYNX_API int lynx_set_option(lynx_ctx* ctx, int option, int value);
 

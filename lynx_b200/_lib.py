@@ -19,6 +19,7 @@ OPT_TC_RAYLEIGH_RITZ = 3
 OPT_COMPACT_GATHER = 4
 OPT_POISSON_DIRECT = 5
 OPT_STENCIL_SHAPE = 6
+OPT_HOST_COPY_BLOCK = 7
 LYNX_ERR_CUDA = 2
 LYNX_ERR_OOM = 3
 LYNX_ERR_CHOL_FAIL = 4

@@ -312,6 +312,7 @@ struct lynx_ctx {
     bool no_tc_gram = false;  // diagnostic switch: FP64 library products for the mixed path
     bool autotune = true;     // time the compiled stencil launch shapes on first use per grid
     int force_shape = -1;     // diagnostic: compiled stencil launch shape used for every launch
+    int host_block = 128;     // columns per block of the pipelined host-to-device copy
     std::map<std::array<long long, 8>, int> pipe_shape;  // chosen launch shape per (type, grid, columns, fused, xold)
     bool fuse_nl = true;      // add the nonlocal term inside the stencil when the spheres are disjoint
     // with fuse_nl: the stencil also writes compact sphere-point copies of its output and the
@@ -2077,8 +2078,9 @@ int lynx_eigensolver_solve_host(lynx_ctx* c, double* psi, double* eig, const dou
     LYNX_TRY(dpsi.ensure(sizeof(double) * (size_t)Nd * nband));
     LYNX_TRY(dv.ensure(sizeof(double) * (size_t)Nd));
     LYNX_CUDA_TRY(cudaMemcpyAsync(dv.p, veff, Nd * 8, cudaMemcpyHostToDevice, c->stream));
-    // Mixed precision, real, pipelined layout: copy psi in blocks of 128 columns on a second
-    // stream; the filter starts on a block as soon as it has landed (see run_filter32).
+    // Mixed precision, real, pipelined layout: copy psi in column blocks (host_block columns, the
+    // remainder last) on a second stream; the filter starts on a block as soon as it has landed
+    // (see run_filter32).
     const bool pipelined = precision == LYNX_PREC_MIXED && pipe_capable<float>(c->nx) && nband >= 256;
     std::vector<cudaEvent_t> evs;
     if (pipelined) {
@@ -2090,7 +2092,7 @@ int lynx_eigensolver_solve_host(lynx_ctx* c, double* psi, double* eig, const dou
         LYNX_CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, start, 0));
         c->col_blocks.clear();
         for (int b0 = 0; b0 < nband;) {
-            const int nb = (nband - b0 <= 192) ? nband - b0 : 128;
+            const int nb = std::min(c->host_block, nband - b0);
             cudaEvent_t ev;
             LYNX_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
             evs.push_back(ev);
@@ -2566,6 +2568,7 @@ extern "C" int lynx_set_option(lynx_ctx* c, int option, int value) {
         case LYNX_OPT_COMPACT_GATHER: c->fuse_compact_gather = value != 0; return LYNX_OK;
         case LYNX_OPT_POISSON_DIRECT: c->poisson_direct = value != 0; return LYNX_OK;
         case LYNX_OPT_STENCIL_SHAPE: c->force_shape = value > 0 ? value - 1 : -1; return LYNX_OK;
+        case LYNX_OPT_HOST_COPY_BLOCK: c->host_block = value > 0 ? value : 128; return LYNX_OK;
         default: set_error("unknown option %d", option); return LYNX_ERR_BAD_ARG;
     }
 }
