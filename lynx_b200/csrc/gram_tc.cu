@@ -320,6 +320,7 @@ __global__ void __launch_bounds__(256) slice_i8_kernel(const SliceArgs a) {
     const float* col = a.y[op] + (long long)j * a.ldy;
     float m = 0.0f;
     bool bad = false;  // fmaxf drops NaN, and slicing would turn it into zeros: flag it instead
+#pragma unroll 4
     for (long long r = r0 + 4 * threadIdx.x; r < rend; r += 4 * blockDim.x) {
         const float4 v = *reinterpret_cast<const float4*>(col + r);
         m = fmaxf(fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y))), fmaxf(fabsf(v.z), fabsf(v.w)));
@@ -341,6 +342,7 @@ __global__ void __launch_bounds__(256) slice_i8_kernel(const SliceArgs a) {
     int8_t* o1 = a.s[3 * op] + (long long)j * a.ldk;
     int8_t* o2 = a.s[3 * op + 1] + (long long)j * a.ldk;
     int8_t* o3 = a.s[3 * op + 2] + (long long)j * a.ldk;
+#pragma unroll 4
     for (long long r = r0 + 4 * threadIdx.x; r < r1; r += 4 * blockDim.x) {
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (r < a.rows) v = *reinterpret_cast<const float4*>(col + r);
@@ -667,9 +669,20 @@ __global__ void __launch_bounds__(256)
     __shared__ int es[32];
     const long long r0 = (long long)blockIdx.x * 32;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int i = w; i < N; i += 8) {
+    // eight loads per warp in flight before their stores (one 128-byte row segment each)
+    for (int i0 = w; i0 < N; i0 += 64) {
         const long long r = r0 + lane;
-        tsm[i * 33 + lane] = (r < rows) ? y[(long long)i * ldy + r] * pow2f(-dcol[i]) : 0.0f;
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + 8 * u;
+            v[u] = (i < N && r < rows) ? y[(long long)i * ldy + r] : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const int i = i0 + 8 * u;
+            if (i < N) tsm[i * 33 + lane] = v[u] * pow2f(-dcol[i]);
+        }
     }
     __syncthreads();
     for (int rr = w; rr < 32; rr += 8) {
