@@ -587,12 +587,13 @@ template <typename Dst, typename Src>
 __global__ void __launch_bounds__(256) repack_kernel(Dst* __restrict__ dst, int dnxp, long long dld,
                                                      const Src* __restrict__ src, int snxp, long long sld, int nx,
                                                      long long nrows) {
-    // one warp per grid row (lanes along x), eight rows per CTA, blockIdx.y = column
-    const long long r = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (r >= nrows) return;
-    const Src* s = src + (long long)blockIdx.y * sld + r * snxp;
-    Dst* d = dst + (long long)blockIdx.y * dld + r * dnxp;
-    for (int xi = threadIdx.x & 31; xi < nx; xi += 32) cvt_val(d[xi], s[xi]);
+    // one warp per grid row (lanes along x), eight rows per CTA and grid-stride over the rows
+    // (a few hundred CTAs per column rather than one per eight rows), blockIdx.y = column
+    for (long long r = (long long)blockIdx.x * 8 + (threadIdx.x >> 5); r < nrows; r += (long long)gridDim.x * 8) {
+        const Src* s = src + (long long)blockIdx.y * sld + r * snxp;
+        Dst* d = dst + (long long)blockIdx.y * dld + r * dnxp;
+        for (int xi = threadIdx.x & 31; xi < nx; xi += 32) cvt_val(d[xi], s[xi]);
+    }
 }
 
 template <typename Dst, typename Src>
@@ -601,7 +602,7 @@ int repack(lynx_ctx* c, Dst* dst, int dnxp, long long dld, const Src* src, int s
     if (nrows == 0 || ncol <= 0) return LYNX_OK;
     for (int c0 = 0; c0 < ncol; c0 += 65535) {  // grid.y limit
         const int nc = std::min(65535, ncol - c0);
-        dim3 grid((unsigned)((nrows + 7) / 8), (unsigned)nc);
+        dim3 grid((unsigned)std::min<long long>((nrows + 7) / 8, 128), (unsigned)nc);
         repack_kernel<Dst, Src><<<grid, 256, 0, c->stream>>>(dst + (long long)c0 * dld, dnxp, dld,
                                                              src + (long long)c0 * sld, snxp, sld, c->nx, nrows);
         count_launch();
