@@ -294,9 +294,11 @@ def test_fused_nonlocal_wide_rows_bitwise(synth_psp8):
             assert np.array_equal(out[key + (prec,)], out[(0, 0, prec)]), (key, prec)
 
 
-def test_host_solve_pipelined_matches_device(system):
+@pytest.mark.parametrize("block", [0, 64, 37])
+def test_host_solve_pipelined_matches_device(system, block):
     """lynx_eigensolver_solve_host copies psi in column blocks on a second stream and filters
-    each block as it lands (mixed precision, >= 256 states): bitwise the device-pointer pass."""
+    each block as it lands (mixed precision, >= 256 states; default blocks of 128 columns, and
+    LYNX_OPT_HOST_COPY_BLOCK 64 and 37): bitwise the device-pointer pass."""
     import ctypes
     from lynx_b200 import _lib
     s = system
@@ -307,9 +309,35 @@ def test_host_solve_pipelined_matches_device(system):
     eig_h = np.zeros(N)
     V = np.ascontiguousarray(s["V"], dtype=np.float64)
     lco = ctypes.c_double()
-    _lib.check(s["ctx"].lib.lynx_eigensolver_solve_host(s["ctx"].handle, _lib.dptr(hp), _lib.dptr(eig_h), _lib.dptr(V),
-                                                       N, s["ctx"].nd, lc, lo, hi, 8, _lib.PREC_MIXED,
-                                                       ctypes.byref(lco)))
+    _lib.check(s["ctx"].lib.lynx_set_option(s["ctx"].handle, _lib.OPT_HOST_COPY_BLOCK, block))
+    try:
+        _lib.check(s["ctx"].lib.lynx_eigensolver_solve_host(s["ctx"].handle, _lib.dptr(hp), _lib.dptr(eig_h),
+                                                           _lib.dptr(V), N, s["ctx"].nd, lc, lo, hi, 8,
+                                                           _lib.PREC_MIXED, ctypes.byref(lco)))
+    finally:
+        _lib.check(s["ctx"].lib.lynx_set_option(s["ctx"].handle, _lib.OPT_HOST_COPY_BLOCK, 0))
     psi_d, eig_d = s["solver"].EigenSolver(s["ctx"], "mixed").solve(psi0, s["V"], lc, lo, hi, 8)
     assert np.array_equal(eig_h, np.asarray(eig_d))
     assert np.array_equal(hp, np.asarray(psi_d))
+
+
+def test_every_stencil_shape_bitwise(system):
+    """Every compiled launch shape of the pipelined stencil and both band splits
+    (LYNX_OPT_STENCIL_SHAPE k = 1..8), with the fused nonlocal term: bitwise the default shape's
+    filter, both precisions."""
+    from lynx_b200 import _lib
+    s = system
+    lo, hi, lc = _bounds(s)
+    X = C.random_orbitals(s["ctx"].nd, 10, seed=95)
+    ctx = s["solver"].Context(s["cell"])
+    ctx.set_nonlocal(P.nonlocal_tables(s["cell"], s["pos"], P.read_psp8(s["synth_psp8"])))
+    es = s["solver"].EigenSolver(ctx)
+    out = {}
+    for k in range(0, 9):
+        _lib.check(ctx.lib.lynx_set_option(ctx.handle, _lib.OPT_STENCIL_SHAPE, k))
+        for prec in ("fp64", "mixed"):
+            out[(k, prec)] = es.chebyshev_filter(X, s["V"], lc, lo, hi, 4, precision=prec)
+    ctx.close()
+    for prec in ("fp64", "mixed"):
+        for k in range(1, 9):
+            assert np.array_equal(out[(k, prec)], out[(0, prec)]), (k, prec)
